@@ -1,0 +1,367 @@
+"""Throughput benchmark: orbit-steps/s of the fixed-step integrators on B200.
+
+Workload (one "step" = one full integration of one batch of orbits):
+  oculomotor model (6 states, 6 parameters), RK4, 2^20 orbits per GPU,
+  parameters uniform within +-50% of the nominal values (seeded), y0 = the
+  reference example's initial state, dt = 1e-3, 10^4 steps, a record every
+  100 steps (101 records, [record][equation][orbit], FP64).
+
+  value     device-resident: inputs already in HBM, one launch per step,
+            CUDA-event time of that launch (L2 flushed between steps).
+  e2e       the same run through the C ABI with host buffers: upload of the
+            inputs from pinned host memory + run with the records copied into
+            pinned host memory, every step (wall clock of the synchronous calls).
+  roofline  counted FP64 operations of the model (224 per RK4 orbit-step,
+            source-level count) over the launch time, against the FP64 FMA
+            issue peak measured on the same GPU by the library's
+            microbenchmark (2 flops per FMA).
+  cpu_baseline  the reference's kernels compiled as C (oracle/_ref), OpenMP over
+            all host cores, on an orbit subsample of the same workload.
+
+--impl reference runs only that CPU implementation of the path (rank 0).
+Under torchrun each rank integrates its own 2^20 orbits (global orbit ids
+offset by rank): weak scaling, no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+NOMINAL = np.array([120.0, 1.5, 0.0045, 0.05, 600.0, 9.0])
+Y0 = np.array([0.0, 0.0, 0.0, 0.0, 0.0, 2.0])
+RK4_OPS_PER_ORBIT_STEP = 224  # 4 x 35 (right-hand side) + 6 x 14 (stage arithmetic)
+METRIC = "orbit-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--orbits", type=int, default=1 << 20)
+    ap.add_argument("--nsteps", type=int, default=10000)
+    ap.add_argument("--ksteps", type=int, default=100)
+    ap.add_argument("--dt", type=float, default=1e-3)
+    ap.add_argument("--solver", default="rk4")
+    ap.add_argument("--precision", default="fp64")
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--cpu-orbits", type=int, default=1 << 15)
+    ap.add_argument("--no-extras", action="store_true", help="skip the companion measurements")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload(n, orbit_offset, seed=2024):
+    """Seeded inputs of orbits [orbit_offset, orbit_offset + n)."""
+    rng = np.random.default_rng([seed, orbit_offset])
+    params = NOMINAL * rng.uniform(0.5, 1.5, (n, 6))
+    return np.zeros(n), np.tile(Y0, (n, 1)), params
+
+
+def config_dict(a, n):
+    return {"workload": "oculomotor-%s-%s" % (a.solver, a.precision), "orbits_per_gpu": n, "nsteps": a.nsteps,
+            "record_every": a.ksteps, "records": a.nsteps // a.ksteps + 1, "dt": a.dt, "neq": 6, "npar": 6,
+            "layout": "[record][equation][orbit]", "l2": "flushed between steps (256 MiB write)"}
+
+
+class ClockSampler:
+    FIELDS = "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown," \
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown," \
+             "clocks_event_reasons.sw_power_cap"
+
+    def __init__(self, device_index):
+        self.dev = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.dev), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_rate(n, a, cores, kind_pref="reference"):
+    """orbit-steps/s of the CPU implementation on the first n orbits."""
+    from oracle.oracle import Oracle, ReferenceBuild
+
+    t0, y0, p = workload(n, 0)
+    solver = {"rk4": 2, "euler": 1, "ie": 3, "im": 4}[a.solver]
+    kw = dict(neq=6, npar=6, dt=a.dt, ksteps=a.ksteps, nchunks=a.nsteps // a.ksteps, nthreads=cores)
+    if kind_pref == "reference" and ReferenceBuild.available("oculomotor", solver):
+        impl, kind = ReferenceBuild("oculomotor", solver), "reference"
+        fn = lambda: impl.run(t0, y0, p, **kw)  # noqa: E731
+    else:
+        impl, kind = Oracle("oculomotor"), "port"
+        fn = lambda: impl.run(solver, t0, y0, p, **kw)  # noqa: E731
+    t = time.perf_counter()
+    fn()
+    secs = time.perf_counter() - t
+    return n * a.nsteps / secs, secs, kind
+
+
+def run_reference_arm(a, rank):
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    n = max(256, a.cpu_orbits // 4)
+    for _ in range(a.warmup):
+        cpu_reference_rate(256, a, cores)
+    vals = []
+    for _ in range(a.steps):
+        v, secs, kind = cpu_reference_rate(n, a, cores)
+        vals.append(v)
+    value = float(np.mean(vals))
+    sample = "%d of %d orbits x %d steps per step, records every %d" % (n, a.orbits, a.nsteps, a.ksteps)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": a.orbits * a.nsteps / value * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_dict(a, a.orbits),
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        run_reference_arm(a, rank)
+        return
+
+    import torch
+
+    import sodecl_b200
+    from sodecl_b200 import Integrator, system_path
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    n = a.orbits
+    offset = rank * n
+    t0, y0, p = workload(n, offset)
+    tspan = a.nsteps * a.dt
+    sim = Integrator(system_path("oculomotor"), a.solver, dt=a.dt, tspan=tspan, ksteps=a.ksteps, neq=6, npar=6,
+                     orbits=n, device=local_rank, precision=a.precision, block=a.block)
+    nchunks = sim.num_chunks
+    assert nchunks * a.ksteps == a.nsteps, (nchunks, a.ksteps, a.nsteps)
+    nrec = nchunks + 1
+    dev = torch.device("cuda", local_rank)
+    stream = torch.cuda.current_stream(dev)
+    t0_d = torch.tensor(t0, device=dev)
+    y0_d = torch.tensor(y0, device=dev)
+    p_d = torch.tensor(p, device=dev)
+    t_d, y_d = t0_d.clone(), y0_d.clone()
+    rec_d = torch.empty((nrec, 6, n), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+
+    def one_launch():
+        sim.launch(t=t_d.data_ptr(), y=y_d.data_ptr(), params=p_d.data_ptr(), records=rec_d.data_ptr(), n=n,
+                   orbit_offset=offset, rec_stride=n, chunk_begin=0, chunk_end=nchunks, write_final=True,
+                   stream=stream.cuda_stream)
+
+    # ---------------- device-resident timing
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(a.steps)]
+    for _ in range(a.warmup):
+        t_d.copy_(t0_d)
+        y_d.copy_(y0_d)
+        one_launch()
+    barrier()
+    with ClockSampler(local_rank) as clocks:
+        barrier()
+        wall0 = time.perf_counter()
+        for i in range(a.steps):
+            t_d.copy_(t0_d)
+            y_d.copy_(y0_d)
+            flush.zero_()
+            starts[i].record(stream)
+            one_launch()
+            ends[i].record(stream)
+        barrier()
+        wall = time.perf_counter() - wall0
+    launch_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms = float(np.mean(launch_ms))
+    if dist is not None:
+        tmax = torch.tensor([ms], device=dev)
+        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
+        ms = float(tmax.item())
+    rec_last = rec_d[-1].cpu().numpy()
+    nan_fraction = float(np.mean(~np.isfinite(rec_last).all(axis=0)))
+    value = world * n * a.nsteps / (ms * 1e-3)
+
+    # ---------------- roofline: counted FP64 ops vs measured FMA issue peak
+    fma_rate, _ = sodecl_b200.fma_peak("fp32" if a.precision == "fp32" else "fp64", device=local_rank)
+    peak_tflops = 2.0 * fma_rate / 1e12
+    achieved = RK4_OPS_PER_ORBIT_STEP * n * a.nsteps / (ms * 1e-3) / 1e12 if a.solver == "rk4" else None
+    roofline = {"bound": "fp64" if a.precision == "fp64" else "fp32", "achieved": achieved, "peak": peak_tflops,
+                "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if achieved else None, "traffic": None,
+                "peak_source": "measured on this GPU: FMA-chain microbenchmark (sodecl_cuda_fma_peak), 2 flops/FMA",
+                "ops_per_orbit_step": RK4_OPS_PER_ORBIT_STEP}
+
+    # ---------------- end to end through the C ABI with host buffers
+    e2e = None
+    h2d = (t0.nbytes + y0.nbytes + p.nbytes)
+    d2h = nrec * 6 * n * 8
+    if not a.no_e2e:
+        del rec_d
+        torch.cuda.empty_cache()
+        host_t = torch.from_numpy(t0).pin_memory()
+        host_y = torch.from_numpy(y0).pin_memory()
+        host_p = torch.from_numpy(p).pin_memory()
+        host_out = torch.empty((nrec, 6, n), dtype=torch.float64, pin_memory=True)
+        from sodecl_b200 import _native as N
+
+        def e2e_step():
+            N.check(N.lib.sodecl_cuda_upload(sim.ctx, host_t.data_ptr(), host_y.data_ptr(), host_p.data_ptr(), None),
+                    sim.ctx)
+            sim.run_into(host_out.data_ptr(), host_out.numel())
+
+        for _ in range(max(1, a.warmup)):
+            e2e_step()
+        barrier()
+        w0 = time.perf_counter()
+        for _ in range(a.steps):
+            e2e_step()
+        barrier()
+        e2e_s = (time.perf_counter() - w0) / a.steps
+        if dist is not None:
+            tm = torch.tensor([e2e_s], device=dev)
+            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+            e2e_s = float(tm.item())
+        e2e = {"value": world * n * a.nsteps / e2e_s, "unit": METRIC, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3, "path": "sodecl_cuda_upload + sodecl_cuda_run, "
+               "pinned host buffers"}
+        assert np.array_equal(host_out[-1].numpy(), rec_last, equal_nan=True)
+
+    # ---------------- companions: stable step, fp32, implicit midpoint
+    extras = {}
+    if not a.no_extras and rank == 0:
+        extras = companions(a, n, dev, stream)
+
+    cpu = None
+    if rank == 0 and world == 1:
+        cores = os.cpu_count() or 1
+        v, secs, kind = cpu_reference_rate(a.cpu_orbits, a, cores)
+        cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": kind,
+               "sample": "%d of %d orbits, all %d steps, records every %d (%.1f s)" % (a.cpu_orbits, n, a.nsteps,
+                                                                                     a.ksteps, secs)}
+    info = sim.kernel_info()
+    if rank == 0:
+        cfg = config_dict(a, n)
+        cfg.update({"parallelism": "orbits sharded, %d per GPU" % n, "block": a.block or 128,
+                    "registers": info["registers"], "nan_fraction_final": nan_fraction})
+        out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps,
+               "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32", "data": "synthetic",
+               "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": a.steps,
+               "clocks": clocks.summary(), "wall_s_timed_region": wall, "launch_ms": launch_ms}
+        out.update(extras)
+        print(json.dumps(out), flush=True)
+    sim.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def companions(a, n, dev, stream):
+    """Same shape, other settings: the stable step dt=1e-5 (RK4 diverges at
+    1e-3 for most parameter draws), FP32, and implicit midpoint."""
+    import torch
+
+    from sodecl_b200 import Integrator, system_path
+
+    out = {}
+    t0, y0, p = workload(n, 0)
+    cases = [("stable_dt_1e-5", a.solver, 1e-5, a.precision), ("fp32", a.solver, a.dt, "fp32"),
+             ("fp32_stable_dt_1e-5", a.solver, 1e-5, "fp32"), ("implicit_midpoint", "im", a.dt, "fp64")]
+    for name, solver, dt, prec in cases:
+        sim = Integrator(system_path("oculomotor"), solver, dt=dt, tspan=a.nsteps * dt, ksteps=a.ksteps, neq=6,
+                         npar=6, orbits=n, precision=prec)
+        nrec = sim.num_records
+        td, yd, pd = torch.tensor(t0, device=dev), torch.tensor(y0, device=dev), torch.tensor(p, device=dev)
+        rec = torch.empty((nrec, 6, n), dtype=torch.float64, device=dev)
+        passes = torch.zeros(n, dtype=torch.int64, device=dev)
+        ms = []
+        for it in range(3):
+            td.copy_(torch.tensor(t0, device=dev))
+            yd.copy_(torch.tensor(y0, device=dev))
+            passes.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(), records=rec.data_ptr(), n=n,
+                       chunk_begin=0, chunk_end=sim.num_chunks, newton_passes=passes.data_ptr(),
+                       stream=stream.cuda_stream)
+            e.record(stream)
+            torch.cuda.synchronize()
+            if it > 0:
+                ms.append(s.elapsed_time(e))
+        last = rec[-1].cpu().numpy()
+        entry = {"value": n * a.nsteps / (np.mean(ms) * 1e-3), "unit": METRIC, "dt": dt, "precision": prec,
+                 "solver": solver, "ms": float(np.mean(ms)),
+                 "nan_fraction_final": float(np.mean(~np.isfinite(last).all(axis=0)))}
+        if solver == "im":
+            entry["newton_passes_per_step"] = float(passes.double().mean().item() / a.nsteps)
+        out[name] = entry
+        sim.close()
+        del rec
+        torch.cuda.empty_cache()
+    return {"companions": out}
+
+
+if __name__ == "__main__":
+    main()

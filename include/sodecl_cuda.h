@@ -1,0 +1,206 @@
+/*
+ * sodecl_cuda.h -- C ABI of libsodecl_cuda.so, the B200 (sm_100a) engine for
+ * SODECL's fixed-step integrators.
+ *
+ * Plain C types only: every caller (the C++ sodecl::sodeclmgr, the Python
+ * module sodecl_interface, ctypes, cgo, ...) binds the same entry points.
+ *
+ * Life cycle, mirroring the reference's sodeclmgr (src/sodeclmgr.cpp):
+ *
+ *   sodecl_cfg_init(&cfg); ...fill cfg...      ctor              :26-83
+ *   sodecl_cuda_create(&cfg, &ctx)             choose_device     :164
+ *   sodecl_cuda_compile(ctx, src, len)         create_kernel_string + build_program
+ *                                                                :374-503, :559-622
+ *   sodecl_cuda_upload(ctx, t0, y0, p, cnt)    set_t0/y0/params + create/write_buffers
+ *                                                                :654-829
+ *   sodecl_cuda_run(ctx, out, len)             run_sode_solver   :921-1035
+ *   sodecl_cuda_destroy(ctx)                   ~sodeclmgr        :88-148
+ *
+ * Status codes: SODECL_OK (0) on success, a negative SODECL_ERR_* otherwise;
+ * sodecl_cuda_last_error() then holds a message.  (The C++ sodeclmgr maps
+ * them to the reference's 1 = success / 0 = failure.)
+ *
+ * Ownership: the library owns all device memory it allocates; the caller owns
+ * every host array and every pointer it passes in.  Threading: a context is
+ * used by one host thread at a time; distinct contexts are independent.
+ */
+#ifndef SODECL_CUDA_H
+#define SODECL_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SODECL_CUDA_ABI_VERSION 1
+
+/* status codes */
+#define SODECL_OK 0
+#define SODECL_ERR_INVALID_ARG (-1)   /* a size, pointer or option is out of range */
+#define SODECL_ERR_COMPILE (-2)       /* NVRTC rejected the program; see the build log */
+#define SODECL_ERR_CUDA (-3)          /* a CUDA runtime call failed */
+#define SODECL_ERR_NO_DEVICE (-4)     /* no CUDA device, or the ordinal does not exist */
+#define SODECL_ERR_STATE (-5)         /* called out of order (e.g. run before upload) */
+#define SODECL_ERR_NO_JACOBIAN (-6)   /* implicit solver, system file has no calc_jacobian */
+#define SODECL_ERR_NO_STOCH (-7)      /* stochastic solver, system file has no sode_system_stoch */
+#define SODECL_ERR_OUT_OF_MEMORY (-8) /* a device or pinned-host allocation failed */
+#define SODECL_ERR_UNSUPPORTED (-9)   /* not available in this build / on this device */
+
+/* solver numbering of the reference's solver_Type (include/solver_Type.hpp:14-20) */
+#define SODECL_STOCHASTIC_EULER 0
+#define SODECL_EULER 1
+#define SODECL_RUNGE_KUTTA 2
+#define SODECL_IMPLICIT_EULER 3
+#define SODECL_IMPLICIT_MIDPOINT 4
+
+#define SODECL_FP64 0
+#define SODECL_FP32 1
+
+/* per-orbit status flags (sodecl_cuda_status) */
+#define SODECL_FLAG_NEWTON_CAP 1   /* some implicit step stopped at newton_max_iter */
+#define SODECL_FLAG_NONFINITE 2    /* a stored record held NaN or Inf */
+
+typedef struct sodecl_ctx sodecl_ctx;
+
+/* Run configuration: the reference's constructor arguments
+ * (include/sodeclmgr.hpp:122-124) plus this library's options. */
+typedef struct sodecl_cfg {
+    int32_t solver;          /* SODECL_STOCHASTIC_EULER .. SODECL_IMPLICIT_MIDPOINT */
+    double dt;               /* step; the program steps with dt printed to 6 significant
+                                digits, as the reference's #define _m_dt_ does */
+    double int_time;         /* tspan: records = count(j < int_time/(dt*kernel_steps)) + 1 */
+    int32_t kernel_steps;    /* steps between records (reference: steps per launch) */
+    int32_t num_equat;
+    int32_t num_params;
+    int32_t num_noi;         /* noise processes; > 0 only with the stochastic solver */
+    int64_t list_size;       /* orbits */
+    int32_t device;          /* CUDA device ordinal */
+    int32_t local_group_size;/* threads per block; 0 = library default */
+    int32_t precision;       /* SODECL_FP64 (default) or SODECL_FP32 */
+    int32_t fmad;            /* 1 (default): allow FMA contraction; 0: exact IEEE op order */
+    double newton_tol;       /* implicit solvers' residual bound; default 1e-7 (sodeclmgr.cpp:425) */
+    int32_t newton_max_iter; /* implicit solvers' pass limit; default 1000 (ie.cl:69, im.cl:65) */
+    int32_t record_f32;      /* device-API records stored as float (sodecl_cuda_launch only) */
+    int32_t min_blocks_per_sm; /* launch-bounds occupancy hint for the compiler; 0 = none */
+} sodecl_cfg;
+
+/* Fills the defaults: Euler, fp64, fmad on, Newton 1e-7 / 1000, device 0. */
+void sodecl_cfg_init(sodecl_cfg *cfg);
+
+/* Validates cfg and makes a context bound to cfg->device.  Needs no GPU
+ * until upload.  Replaces sodeclmgr::sodeclmgr + choose_device
+ * (src/sodeclmgr.cpp:26-83, :164). */
+int sodecl_cuda_create(const sodecl_cfg *cfg, sodecl_ctx **out);
+
+/* Builds the program for the user's system file (OpenCL C text, as the
+ * reference reads it from disk) with NVRTC for sm_100a.  Needs no GPU.
+ * Replaces create_kernel_string/create_program/build_program
+ * (src/sodeclmgr.cpp:374-622). */
+int sodecl_cuda_compile(sodecl_ctx *ctx, const char *system_src, size_t len);
+
+/* Copies the initial state to the device: t0[list_size], y0[list_size][num_equat],
+ * params[list_size][num_params] (orbit-major, as the reference's host arrays),
+ * counters[list_size] the noise draw counters (stochastic solver; NULL draws
+ * them as the reference does, U(-1e11, 1e11), from a generator seeded with 0).
+ * Replaces set_t0/set_y0/set_params + create_buffers/write_buffers
+ * (src/sodeclmgr.cpp:654-829, counters :48-59). */
+int sodecl_cuda_upload(sodecl_ctx *ctx, const double *t0, const double *y0, const double *params,
+                       const double *counters);
+
+/* Records one run produces: launches + 1 (src/sodeclmgr.cpp:951, :998). */
+int64_t sodecl_cuda_num_records(const sodecl_ctx *ctx);
+
+/* Integrates every orbit over int_time from the current device state and
+ * writes num_records() records of num_equat x list_size doubles to `out` in
+ * the reference's [record][equation][orbit] order (src/sodeclmgr.cpp:980-994).
+ * `out` may be host memory (pageable or pinned) or device memory; NULL
+ * discards the records (output_Type::None).  out_len is the capacity in
+ * doubles.  The state stays on the device, so a second call continues from
+ * where the first stopped.  Replaces run_sode_solver (:921-1035). */
+int sodecl_cuda_run(sodecl_ctx *ctx, double *out, int64_t out_len);
+
+/* Copies the current state back: any pointer may be NULL. */
+int sodecl_cuda_download_state(sodecl_ctx *ctx, double *t, double *y, double *counters);
+
+/* Per-orbit status accumulated since upload: Newton passes taken and
+ * SODECL_FLAG_* bits.  Either pointer may be NULL.  (No counterpart in the
+ * reference, which reports nothing per orbit.) */
+int sodecl_cuda_status(sodecl_ctx *ctx, int64_t *newton_passes, int32_t *flags);
+
+/* Device time of the last run's kernels in milliseconds (CUDA events). */
+int sodecl_cuda_last_run_ms(const sodecl_ctx *ctx, double *kernel_ms, double *total_ms);
+
+/* Copies the last error message / the NVRTC build log (NUL-terminated,
+ * truncated to n bytes).  Return the full length. */
+size_t sodecl_cuda_last_error(const sodecl_ctx *ctx, char *buf, size_t n);
+size_t sodecl_cuda_build_log(const sodecl_ctx *ctx, char *buf, size_t n);
+
+/* The generated program text (for debugging; the reference writes it to
+ * Generated_kernel.cl, src/sodeclmgr.cpp:498-500). */
+size_t sodecl_cuda_program_source(const sodecl_ctx *ctx, char *buf, size_t n);
+
+void sodecl_cuda_destroy(sodecl_ctx *ctx);
+
+const char *sodecl_cuda_strerror(int status);
+int sodecl_cuda_abi_version(void);
+int sodecl_cuda_device_count(int *count);
+
+/* ---- device-buffer path (torch / custom callers; no host copies) ------- */
+
+/* One launch over caller-owned device buffers, on the caller's stream
+ * (NULL = the legacy default stream).  Pointers are device pointers:
+ * t[n], y[n][neq], params[n][npar] (doubles, in/out except params),
+ * counters[n] (stochastic solver), records = base of a window
+ * [record][neq][rec_stride] of double (or float with cfg.record_f32) whose
+ * first row is record rec_first.  Runs record intervals
+ * [chunk_begin, chunk_end), storing each interval's starting state, and the
+ * final state as record chunk_end if write_final.  newton_passes/flags
+ * (nullable) accumulate.  The context must be compiled; no upload needed. */
+typedef struct sodecl_launch {
+    double *t;
+    double *y;
+    const double *params;
+    double *counters;
+    void *records;
+    int64_t n;
+    int64_t orbit_offset;   /* global orbit index of orbit 0 (noise stream) */
+    int64_t rec_stride;
+    int64_t rec_col0;
+    int32_t chunk_begin;
+    int32_t chunk_end;
+    int32_t rec_first;
+    int32_t write_final;
+    int64_t *newton_passes;
+    int32_t *flags;
+} sodecl_launch;
+
+int sodecl_cuda_launch(sodecl_ctx *ctx, const sodecl_launch *launch, void *stream);
+
+/* Kernel resources of the compiled program on its device (registers per
+ * thread, local memory bytes per thread, max threads per block).  Needs a GPU. */
+int sodecl_cuda_kernel_info(sodecl_ctx *ctx, int *regs, int *local_bytes, int *max_threads);
+
+/* ---- test and measurement helpers -------------------------------------- */
+
+/* The Euler-Maruyama noise stream computed on the GPU by the same device
+ * code the solver uses.  For each of n orbits (global ids gids[i], starting
+ * draw counters counters[i]) and nsteps steps: Gaussian increments
+ * normals[(i*nsteps + s)*nnoi + k] for step `dt_program` (the printed step),
+ * and optionally the raw Threefry words and (0,1) doubles of every draw,
+ * words/u01[((i*nsteps + s)*ncalls + c)*2 + {0,1}], ncalls = (nnoi+1)/2.
+ * Host pointers. */
+int sodecl_cuda_noise_stream(int device, const int64_t *gids, const double *counters, int64_t n, int32_t nnoi,
+                             double dt_program, int64_t nsteps, double *normals, uint64_t *words, double *u01);
+
+/* Issue-rate microbenchmark of the FP64 (precision 0) or FP32 (1) FMA pipe:
+ * independent FMA chains on every SM, timed with CUDA events.  Writes the
+ * FMA instructions per second summed over all lanes (one FMA = 2 flops). */
+int sodecl_cuda_fma_peak(int device, int32_t precision, double *fma_per_s, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SODECL_CUDA_H */

@@ -1,0 +1,88 @@
+// sodeclmgr.hpp -- drop-in C++ manager for the CUDA engine.
+//
+// Same public surface as the reference's sodecl::sodeclmgr
+// (include/sodeclmgr.hpp:27-369 of the reference): constructor, choose_device,
+// set_local_group_size, set_t0/set_y0/set_params, setup_sode_solver,
+// run_sode_solver, m_output.  The OpenCL types become plain C++ types
+// (cl_uint -> unsigned, cl_double -> double); the enums keep their names and
+// values.  Everything below the public methods is the C ABI of sodecl_cuda.h.
+#ifndef SODECL_B200_SODECLMGR_HPP
+#define SODECL_B200_SODECLMGR_HPP
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "sodecl_cuda.h"
+
+namespace sodecl {
+
+// include/solver_Type.hpp:14-20 of the reference
+enum class solver_Type { StochasticEuler = 0, Euler = 1, RungeKutta = 2, ImplicitEuler = 3, ImplicitMidpoint = 4 };
+
+// include/output_Type.hpp:14-18 of the reference
+enum class output_Type { None = 0, Array = 1, File = 2 };
+
+// include/device_Type.hpp:14-19 of the reference (OpenCL device-type bits);
+// accepted for source compatibility, CUDA devices are chosen by ordinal.
+enum class device_Type : uint64_t { ALL = 0xFFFFFFFFull, CPU = 1ull << 1, GPU = 1ull << 2, ACCELERATOR = 1ull << 3 };
+
+class sodeclmgr {
+  public:
+    std::vector<double> m_output;  // records, [record][equation][orbit]
+    int m_output_size = 0;
+
+    // kernel_path_str is accepted and ignored (the solvers are built in);
+    // sode_system_str is the path of the system file, read at setup.
+    sodeclmgr(std::string kernel_path_str, char *sode_system_str, solver_Type solver, double dt, double int_time,
+              int kernel_steps, int num_equat, int num_params, int num_noi, int list_size, output_Type output_type);
+    ~sodeclmgr();
+    sodeclmgr(const sodeclmgr &) = delete;
+    sodeclmgr &operator=(const sodeclmgr &) = delete;
+
+    // platform_num and device_type are ignored; device_num is the CUDA ordinal.
+    // Returns 1 if the device exists, 0 otherwise.
+    int choose_device(unsigned platform_num, device_Type device_type, unsigned device_num);
+
+    // Threads per CUDA block (0 = library default).
+    void set_local_group_size(int local_group_size);
+
+    // Non-owning: the arrays must stay valid until setup_sode_solver returns.
+    void set_t0(double *t0);
+    void set_y0(double *y0);
+    void set_params(double *params);
+
+    // Reads a whitespace-separated text file / raw doubles into `data`.
+    int read_binary_data_from_file(char *filename, double *data);
+    int read_data_from_file(char *filename, double *data);
+
+    // 1 = success, 0 = failure, as the reference.
+    int setup_sode_solver();
+    int run_sode_solver();
+
+    // ---- additions (no counterpart in the reference) ----
+    // Noise draw counters, list_size doubles (non-owning, read at setup);
+    // without them the counters are drawn as the reference draws them.
+    void set_noise_counters(const double *counters);
+    void set_newton(double tol, int max_iter);
+    void set_precision(int precision);  // SODECL_FP64 or SODECL_FP32
+    void set_fmad(bool on);
+    sodecl_ctx *context() const { return m_ctx; }
+    const std::string &last_error() const { return m_error; }
+
+  private:
+    sodecl_cfg m_cfg{};
+    std::string m_system_path;
+    output_Type m_output_type;
+    std::string m_outputfile_str = "sodecloutput.bin";
+    double *m_t0 = nullptr;
+    double *m_y0 = nullptr;
+    double *m_params = nullptr;
+    const double *m_counters = nullptr;
+    sodecl_ctx *m_ctx = nullptr;
+    std::string m_error;
+};
+
+}  // namespace sodecl
+
+#endif

@@ -1,0 +1,155 @@
+// Statically compiled (nvcc, sm_100a) kernels of libsodecl_cuda:
+//  * the Euler-Maruyama noise stream, computed by the same device code the
+//    NVRTC solver programs embed (device/threefry.cuh), for bit-exactness
+//    tests against the CPU generator;
+//  * an FMA issue-rate microbenchmark, the denominator of the FP64/FP32
+//    "fraction of issue peak" figures.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "device/threefry.cuh"
+#include "sodecl_cuda.h"
+
+namespace {
+
+__global__ void noise_stream_kernel(const long long *gids, const double *counters, long long n, int nnoi, double dt,
+                                    long long nsteps, double *normals, unsigned long long *words, double *u01)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int ncalls = (nnoi + 1) / 2;
+    const double sqrt_h = sqrt(dt);
+    const unsigned long long gid = (unsigned long long)gids[i];
+    double counter = counters[i];
+    for (long long s = 0; s < nsteps; ++s) {
+        for (int c = 0; c < ncalls; ++c) {
+            unsigned long long w0, w1;
+            sodecl_threefry2x64_20(gid, sodecl_counter_word(counter), SODECL_TF_KEY0, SODECL_TF_KEY1, w0, w1);
+            counter = counter + 1;
+            const long long draw = (i * nsteps + s) * ncalls + c;
+            if (words) {
+                words[2 * draw] = w0;
+                words[2 * draw + 1] = w1;
+            }
+            if (u01) {
+                u01[2 * draw] = sodecl_u01_open_open(w0);
+                u01[2 * draw + 1] = sodecl_u01_open_open(w1);
+            }
+            double n0, n1;
+            sodecl_gaussian_pair<double>(w0, w1, sqrt_h, n0, n1);
+            const long long base = (i * nsteps + s) * nnoi;
+            normals[base + 2 * c] = n0;
+            if (2 * c + 1 < nnoi) normals[base + 2 * c + 1] = n1;
+        }
+    }
+}
+
+// Eight independent FMA chains per thread, unrolled; every SM full of warps.
+template <class T>
+__global__ void __launch_bounds__(256) fma_chains_kernel(T *sink, int iters, T a, T b)
+{
+    T x0 = (T)threadIdx.x * (T)1e-3, x1 = x0 + (T)1, x2 = x0 + (T)2, x3 = x0 + (T)3;
+    T x4 = x0 + (T)4, x5 = x0 + (T)5, x6 = x0 + (T)6, x7 = x0 + (T)7;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            x0 = fma(x0, a, b); x1 = fma(x1, a, b); x2 = fma(x2, a, b); x3 = fma(x3, a, b);
+            x4 = fma(x4, a, b); x5 = fma(x5, a, b); x6 = fma(x6, a, b); x7 = fma(x7, a, b);
+        }
+    }
+    const T s = ((x0 + x1) + (x2 + x3)) + ((x4 + x5) + (x6 + x7));
+    if (s == (T)-12345.0) sink[blockIdx.x * blockDim.x + threadIdx.x] = s;  // never true; keeps the chains live
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) { if (cudaGetDevice(&prev) != cudaSuccess) prev = -1; cudaSetDevice(dev); }
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
+
+template <class T>
+int run_fma_peak(int device, double *fma_per_s, double *ms_out)
+{
+    DeviceGuard guard(device);
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { cudaGetLastError(); return SODECL_ERR_NO_DEVICE; }
+    const int block = 256;
+    const int blocks = prop.multiProcessorCount * 8;
+    const int iters = 1 << 14;
+    T *sink = nullptr;
+    if (cudaMalloc(&sink, sizeof(T) * (size_t)blocks * block) != cudaSuccess) { cudaGetLastError(); return SODECL_ERR_OUT_OF_MEMORY; }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const T a = (T)0.999999, b = (T)1e-7;
+    fma_chains_kernel<T><<<blocks, block>>>(sink, iters / 8, a, b);  // warm-up
+    cudaEventRecord(e0);
+    fma_chains_kernel<T><<<blocks, block>>>(sink, iters, a, b);
+    cudaEventRecord(e1);
+    cudaError_t err = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sink);
+    if (err != cudaSuccess) { cudaGetLastError(); return SODECL_ERR_CUDA; }
+    const double fmas = (double)blocks * block * (double)iters * 4.0 * 8.0;
+    if (fma_per_s) *fma_per_s = fmas / (ms * 1e-3);
+    if (ms_out) *ms_out = ms;
+    return SODECL_OK;
+}
+
+}  // namespace
+
+extern "C" int sodecl_cuda_noise_stream(int device, const int64_t *gids, const double *counters, int64_t n, int32_t nnoi,
+                                        double dt_program, int64_t nsteps, double *normals, uint64_t *words, double *u01)
+{
+    if (!gids || !counters || !normals || n < 1 || nnoi < 1 || nsteps < 1 || !(dt_program > 0)) return SODECL_ERR_INVALID_ARG;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) { cudaGetLastError(); return SODECL_ERR_NO_DEVICE; }
+    DeviceGuard guard(device);
+    const int ncalls = (nnoi + 1) / 2;
+    const size_t n_norm = (size_t)n * nsteps * nnoi, n_draw = (size_t)n * nsteps * ncalls * 2;
+    long long *d_gid = nullptr;
+    double *d_cnt = nullptr, *d_norm = nullptr, *d_u01 = nullptr;
+    unsigned long long *d_words = nullptr;
+    int rc = SODECL_OK;
+    auto check = [&](cudaError_t e) { if (e != cudaSuccess && rc == SODECL_OK) { rc = (e == cudaErrorMemoryAllocation) ? SODECL_ERR_OUT_OF_MEMORY : SODECL_ERR_CUDA; cudaGetLastError(); } };
+    check(cudaMalloc(&d_gid, n * sizeof(long long)));
+    check(cudaMalloc(&d_cnt, n * sizeof(double)));
+    check(cudaMalloc(&d_norm, n_norm * sizeof(double)));
+    if (words) check(cudaMalloc(&d_words, n_draw * sizeof(unsigned long long)));
+    if (u01) check(cudaMalloc(&d_u01, n_draw * sizeof(double)));
+    if (rc == SODECL_OK) {
+        check(cudaMemcpy(d_gid, gids, n * sizeof(long long), cudaMemcpyHostToDevice));
+        check(cudaMemcpy(d_cnt, counters, n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    if (rc == SODECL_OK) {
+        const int block = 128;
+        noise_stream_kernel<<<(unsigned)((n + block - 1) / block), block>>>(d_gid, d_cnt, n, nnoi, dt_program, nsteps, d_norm, d_words, d_u01);
+        check(cudaGetLastError());
+        check(cudaDeviceSynchronize());
+    }
+    if (rc == SODECL_OK) {
+        check(cudaMemcpy(normals, d_norm, n_norm * sizeof(double), cudaMemcpyDeviceToHost));
+        if (words) check(cudaMemcpy(words, d_words, n_draw * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+        if (u01) check(cudaMemcpy(u01, d_u01, n_draw * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    cudaFree(d_gid);
+    cudaFree(d_cnt);
+    cudaFree(d_norm);
+    cudaFree(d_words);
+    cudaFree(d_u01);
+    return rc;
+}
+
+extern "C" int sodecl_cuda_fma_peak(int device, int32_t precision, double *fma_per_s, double *ms)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) { cudaGetLastError(); return SODECL_ERR_NO_DEVICE; }
+    if (precision == SODECL_FP64) return run_fma_peak<double>(device, fma_per_s, ms);
+    if (precision == SODECL_FP32) return run_fma_peak<float>(device, fma_per_s, ms);
+    return SODECL_ERR_INVALID_ARG;
+}

@@ -1,0 +1,60 @@
+// NVRTC front end: turns a SODECL system file into an sm_100a cubin.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace sodecl_b200 {
+
+struct ProgramSpec {
+    int solver = 1;          // solver_Type numbering
+    int num_equat = 0;
+    int num_params = 0;
+    int num_noi = 0;
+    int64_t list_size = 0;
+    int kernel_steps = 1;
+    double dt = 0.0;         // user dt; printed like the reference
+    bool fp32 = false;
+    bool fmad = true;
+    bool record_f32 = false;
+    double newton_tol = 1e-7;
+    int newton_max_iter = 1000;
+    int block_max = 256;
+    int min_blocks = 0;
+};
+
+struct Program {
+    std::string source;      // full program text handed to NVRTC
+    std::string log;         // NVRTC log (with ptxas resource usage)
+    std::vector<char> cubin;
+    std::string kernel_name = "sodecl_orbits";
+};
+
+// What the system file provides.
+struct SystemTraits {
+    bool has_system = false;
+    bool has_jacobian = false;
+    bool has_stoch = false;
+    bool uses_listsize = false;
+};
+
+SystemTraits inspect_system(const std::string &src);
+
+// `dt` exactly as the reference writes it into `#define _m_dt_`: a default
+// std::ostream, i.e. %g with 6 significant digits (src/sodeclmgr.cpp:356-367).
+std::string print_like_reference(double x);
+
+// Every unsuffixed floating literal outside comments, strings and character
+// constants gets an `f` suffix (fp32 programs).
+std::string suffix_float_literals(const std::string &src);
+
+// Assembles the program text.
+std::string assemble(const ProgramSpec &spec, const std::string &system_src, const SystemTraits &traits);
+
+// Compiles (or returns from the process-wide cache) the program.  Throws
+// std::runtime_error with the NVRTC log on failure.
+std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string &system_src);
+
+}  // namespace sodecl_b200

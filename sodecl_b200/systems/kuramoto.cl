@@ -1,0 +1,57 @@
+/*
+ * Kuramoto model of N = _numeq_ coupled phase oscillators:
+ *
+ *   d(theta_i)/dt = omega_i + (K/N) * sum_j sin(theta_j - theta_i)
+ *
+ * with the sum over every j, i included.  Parameters p = [K, omega_1..N],
+ * followed by N noise amplitudes sigma_1..N when the system is integrated
+ * with Euler-Maruyama (additive noise sigma_i * dW_i).
+ *
+ * `sode_system` and `sode_system_stoch` evaluate in the same floating-point
+ * order as the reference's examples/kuramoto.cl (:3-16, :18-24).
+ * The reference ships no Jacobian for this model; `calc_jacobian` below is
+ * this library's addition so the implicit solvers can integrate it:
+ *   J_ij = (K/N) cos(theta_j - theta_i)               (j != i)
+ *   J_ii = -(K/N) sum_{j != i} cos(theta_j - theta_i)
+ */
+
+void sode_system(double t, double y[_numeq_], double yout[_numeq_], double p[_numpar_])
+{
+	for (int i = 0; i < _numeq_; i++)
+	{
+		double coupling = 0;
+		for (int j = 0; j < _numeq_; j++)
+		{
+			coupling = coupling + (sin(y[j] - y[i]));
+		}
+		coupling = coupling * (double)(p[0] / (double)(_numeq_));
+		yout[i] = coupling + p[i + 1];
+	}
+}
+
+void calc_jacobian(double y[_numeq_], double jac[_numeq_][_numeq_], double p[_numpar_])
+{
+	double scale = (double)(p[0] / (double)(_numeq_));
+	for (int i = 0; i < _numeq_; i++)
+	{
+		double diag = 0;
+		for (int j = 0; j < _numeq_; j++)
+		{
+			double c = scale * cos(y[j] - y[i]);
+			jac[i][j] = c;
+			if (j != i)
+			{
+				diag = diag - c;
+			}
+		}
+		jac[i][i] = diag;
+	}
+}
+
+void sode_system_stoch(double t, double y[_numeq_], double stoch[_numeq_], double p[_numpar_], double noise[_numnoi_])
+{
+	for (int i = 0; i < _numeq_; i++)
+	{
+		stoch[i] = p[_numpar_ - _numnoi_ + i] * noise[i];
+	}
+}

@@ -1,0 +1,112 @@
+/*
+ * Oculomotor (saccadic eye-movement) model: 6 states, 6 parameters,
+ * optionally 2 noise processes.  A SODECL system file: it defines the
+ * right-hand side `sode_system`, the analytic Jacobian `calc_jacobian`
+ * (needed by the implicit solvers) and the diffusion term
+ * `sode_system_stoch` (needed by Euler-Maruyama).
+ *
+ * State y = [g, u, n, r, l, m]:
+ *   g  eye position            u  eye velocity
+ *   n  neural integrator       r  right burst neuron
+ *   l  left burst neuron       m  motor error
+ * Parameters p = [alpha, beta, tau, gamma, alpha_t, beta_t] of the burst
+ * non-linearity (nominal 120, 1.5, 0.0045, 0.05, 600, 9), followed by the
+ * noise amplitudes when noise processes are used.
+ *
+ * Same model and the same floating-point evaluation order as the
+ * reference's examples/oculomotor.cl (sburstf :5-20, dsburstf :22-36,
+ * calc_jacobian :38-81, sode_system :83-97, sode_system_stoch :99-112),
+ * so trajectories agree with the reference to the last bits.
+ */
+
+#define OCM_T1 0.15
+#define OCM_T2 0.012
+#define OCM_TN 25.00
+/* plant gains, folded at compile time */
+#define OCM_VEL_GAIN ((1.00 / OCM_T1) + (1.00 / OCM_T2))
+#define OCM_POS_GAIN (1.00 / (OCM_T1 * OCM_T2))
+
+/* burst-neuron firing-rate non-linearity */
+double ocm_burst(double x, double a, double b, double at, double bt)
+{
+	double rate = 0;
+	if (x > 0)
+	{
+		rate = (at * (1.00 - exp(-x / bt)));
+	}
+	else
+	{
+		rate = (-(a / b) * x * exp(x / b));
+	}
+	return rate;
+}
+
+/* d(ocm_burst)/dx */
+double ocm_burst_slope(double x, double a, double b, double at, double bt)
+{
+	double slope = 0;
+	if (x > 0)
+	{
+		slope = (at * exp(-x / bt)) / bt;
+	}
+	else
+	{
+		slope = -((a * exp(x / b)) / b + (a * x * exp(x / b)) / (b * b));
+	}
+	return slope;
+}
+
+void sode_system(double t, double y[_numeq_], double yout[_numeq_], double p[_numpar_])
+{
+	double drive = y[3] - y[4];
+	yout[0] = y[1];
+	yout[1] = -(OCM_VEL_GAIN * y[1]) - (OCM_POS_GAIN * y[0]) + (OCM_POS_GAIN * y[2]) + OCM_VEL_GAIN * drive;
+	yout[2] = -(y[2] / OCM_TN) + drive;
+	yout[3] = (1.00 / p[2]) * (-y[3] - (p[3] * y[3] * y[4] * y[4]) + ocm_burst(y[5], p[0], p[1], p[4], p[5]));
+	yout[4] = (1.00 / p[2]) * (-y[4] - (p[3] * y[4] * y[3] * y[3]) + ocm_burst(-y[5], p[0], p[1], p[4], p[5]));
+	yout[5] = -drive;
+}
+
+void calc_jacobian(double y[_numeq_], double jac[_numeq_][_numeq_], double p[_numpar_])
+{
+	int i, j;
+	for (i = 0; i < 6; i++)
+	{
+		for (j = 0; j < 6; j++)
+		{
+			jac[i][j] = 0;
+		}
+	}
+	jac[0][1] = 1;
+
+	jac[1][0] = -1 / (OCM_T1 * OCM_T2);
+	jac[1][1] = -(1 / OCM_T1) - (1 / OCM_T2);
+	jac[1][2] = 1 / (OCM_T1 * OCM_T2);
+	jac[1][3] = (1 / OCM_T1) + (1 / OCM_T2);
+	jac[1][4] = -(1 / OCM_T1) - (1 / OCM_T2);
+
+	jac[2][2] = -1 / OCM_TN;
+	jac[2][3] = 1;
+	jac[2][4] = -1;
+
+	jac[3][3] = -(p[3] * (y[4] * y[4]) + 1) / p[2];
+	jac[3][4] = -(2 * p[3] * y[4] * y[3]) / p[2];
+	jac[3][5] = ocm_burst_slope(y[5], p[0], p[1], p[4], p[5]) / p[2];
+
+	jac[4][3] = -(2 * p[3] * y[4] * y[3]) / p[2];
+	jac[4][4] = -(p[3] * (y[3] * y[3]) + 1) / p[2];
+	jac[4][5] = ocm_burst_slope(-y[5], p[0], p[1], p[4], p[5]) / p[2];
+
+	jac[5][3] = -1;
+	jac[5][4] = 1;
+}
+
+void sode_system_stoch(double t, double y[_numeq_], double stoch[_numeq_], double p[_numpar_], double noise[_numnoi_])
+{
+	int k;
+	for (k = 0; k < 6; k++)
+	{
+		stoch[k] = 0;
+	}
+	stoch[1] = OCM_VEL_GAIN * (y[3] - y[4]) * p[_numpar_ - _numnoi_ + 0] * noise[0] + p[_numpar_ - _numnoi_ + 1] * noise[1];
+}

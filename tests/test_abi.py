@@ -1,0 +1,198 @@
+"""The C ABI library on a machine without a GPU: it loads, exports every entry
+point include/sodecl_cuda.h declares, validates configurations, and builds
+programs with NVRTC (which needs no device).  Failure paths return the
+documented status codes."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from sodecl_b200 import _native as N
+from sodecl_b200 import Integrator, system_path
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(REPO, "include", "sodecl_cuda.h")
+REFERENCE_ROOT = os.environ.get("SODECL_REFERENCE_ROOT", "/root/reference")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", " ", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sodecl_\w+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    names = declared_functions()
+    assert len(names) >= 20
+    out = subprocess.run(["nm", "-D", "--defined-only", N.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(line.split()[-1] for line in out.splitlines() if line.strip())
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    # and the ctypes binding declares each of them
+    assert sorted(N.SIGNATURES) == names
+
+
+def test_abi_version_and_strerror():
+    assert N.lib.sodecl_cuda_abi_version() == 1
+    assert N.lib.sodecl_cuda_strerror(N.ERR_NO_JACOBIAN).decode().startswith("implicit solver")
+
+
+def _cfg(**kw):
+    cfg = N.Cfg()
+    N.lib.sodecl_cfg_init(C.byref(cfg))
+    base = dict(solver=2, dt=1e-3, int_time=1.0, kernel_steps=10, num_equat=6, num_params=6, list_size=8)
+    base.update(kw)
+    for k, v in base.items():
+        setattr(cfg, k, v)
+    return cfg
+
+
+def _create(**kw):
+    ctx = C.c_void_p()
+    rc = N.lib.sodecl_cuda_create(C.byref(_cfg(**kw)), C.byref(ctx))
+    return rc, ctx
+
+
+def test_cfg_defaults():
+    cfg = N.Cfg()
+    N.lib.sodecl_cfg_init(C.byref(cfg))
+    assert cfg.solver == N.EULER and cfg.fmad == 1 and cfg.precision == N.FP64
+    assert cfg.newton_tol == 1e-7 and cfg.newton_max_iter == 1000
+
+
+@pytest.mark.parametrize("bad", [dict(solver=5), dict(solver=-1), dict(num_equat=0), dict(list_size=0),
+                                 dict(dt=0.0), dict(dt=float("nan")), dict(kernel_steps=0),
+                                 dict(solver=0, num_noi=0), dict(precision=2), dict(int_time=-1.0),
+                                 dict(local_group_size=2048), dict(dt=1e-12, int_time=1.0, kernel_steps=1)])
+def test_create_rejects_invalid_configuration(bad):
+    rc, ctx = _create(**bad)
+    assert rc == N.ERR_INVALID_ARG
+    assert not ctx.value
+
+
+def test_record_count():
+    rc, ctx = _create(dt=1e-6, int_time=0.1, kernel_steps=400)
+    assert rc == N.OK
+    assert N.lib.sodecl_cuda_num_records(ctx) == 252
+    N.lib.sodecl_cuda_destroy(ctx)
+
+
+def _compile(ctx, src):
+    b = src.encode() if isinstance(src, str) else src
+    return N.lib.sodecl_cuda_compile(ctx, b, len(b))
+
+
+@pytest.mark.parametrize("solver", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_compile_every_solver_without_gpu(solver, precision):
+    nnoi = 2 if solver == 0 else 0
+    rc, ctx = _create(solver=solver, num_noi=nnoi, num_params=6 + nnoi, precision=precision)
+    assert rc == N.OK
+    src = open(system_path("oculomotor")).read()
+    assert _compile(ctx, src) == N.OK, N.last_error(ctx)
+    text = N.program_source(ctx)
+    # the reference's program defines, same names and printed values
+    for line in ("#define _numnoi_ %d" % nnoi, "#define _numsteps_ 10", "#define _numeq_ 6",
+                 "#define _numpar_ %d" % (6 + nnoi)):
+        assert line in text
+    assert ("#define _m_dt_ 0.001f" if precision else "#define _m_dt_ 0.001\n") in text
+    assert "ptxas" in N.build_log(ctx)  # resource usage is reported
+    N.lib.sodecl_cuda_destroy(ctx)
+
+
+def test_fp32_program_rewrites_literals():
+    rc, ctx = _create(precision=1)
+    assert _compile(ctx, open(system_path("oculomotor")).read()) == N.OK
+    text = N.program_source(ctx)
+    assert "#define double float" in text
+    assert "#define OCM_T1 0.15f" in text and "(1.00f / p[2])" in text
+    assert "/* burst-neuron firing-rate non-linearity */" in text  # comments untouched
+    N.lib.sodecl_cuda_destroy(ctx)
+
+
+def test_zero_size_parameter_bounds_are_relaxed():
+    # the system file declares `double noise[_numnoi_]`; _numnoi_ is 0 for ODE runs
+    rc, ctx = _create(solver=2)
+    assert _compile(ctx, open(system_path("oculomotor")).read()) == N.OK
+    text = N.program_source(ctx)
+    assert re.search(r"double noise\[\s*\]", text)
+    assert re.search(r"double jac\[\s*\]\[_numeq_\]", text)
+    N.lib.sodecl_cuda_destroy(ctx)
+
+
+def test_missing_jacobian_and_stochastic_term():
+    kura = open(system_path("kuramoto")).read()
+    no_jac = re.sub(r"void calc_jacobian.*?\n}\n", "", kura, flags=re.S)
+    assert "void calc_jacobian" not in no_jac
+    rc, ctx = _create(solver=3, num_equat=4, num_params=5)
+    assert _compile(ctx, no_jac) == N.ERR_NO_JACOBIAN
+    assert "calc_jacobian" in N.last_error(ctx)
+    N.lib.sodecl_cuda_destroy(ctx)
+    no_stoch = re.sub(r"void sode_system_stoch.*?\n}\n", "", kura, flags=re.S)
+    rc, ctx = _create(solver=0, num_equat=4, num_params=9, num_noi=4)
+    assert _compile(ctx, no_stoch) == N.ERR_NO_STOCH
+    N.lib.sodecl_cuda_destroy(ctx)
+
+
+def test_compile_error_reports_nvrtc_log():
+    rc, ctx = _create()
+    bad = "void sode_system(double t, double y[_numeq_], double yout[_numeq_], double p[_numpar_]) { yout[0] = y[0] +; }"
+    assert _compile(ctx, bad) == N.ERR_COMPILE
+    assert "error" in N.last_error(ctx)
+    assert _compile(ctx, "int nothing_here;") == N.ERR_COMPILE  # no sode_system
+    N.lib.sodecl_cuda_destroy(ctx)
+
+
+def test_out_of_order_calls():
+    rc, ctx = _create()
+    out = np.zeros(10)
+    assert N.lib.sodecl_cuda_run(ctx, out.ctypes.data, out.size) == N.ERR_STATE
+    assert N.lib.sodecl_cuda_download_state(ctx, None, None, None) == N.ERR_STATE
+    z = np.zeros(48)
+    # upload before compile
+    assert N.lib.sodecl_cuda_upload(ctx, z.ctypes.data, z.ctypes.data, z.ctypes.data, None) == N.ERR_STATE
+    assert N.lib.sodecl_cuda_upload(None, None, None, None, None) == N.ERR_INVALID_ARG
+    N.lib.sodecl_cuda_destroy(ctx)
+    N.lib.sodecl_cuda_destroy(None)
+
+
+@pytest.mark.skipif(N.device_count() > 0, reason="checks the no-device path")
+def test_no_device_is_reported():
+    sim = Integrator(system_path("oculomotor"), "rk4", dt=1e-3, tspan=0.01, ksteps=10, neq=6, npar=6, orbits=4)
+    with pytest.raises(N.SodeclError) as e:
+        sim.upload(np.zeros(4), np.zeros(24), np.ones(24))
+    assert e.value.status == N.ERR_NO_DEVICE
+    assert N.lib.sodecl_cuda_noise_stream(0, np.zeros(1, np.int64).ctypes.data, np.zeros(1).ctypes.data, 1, 2, 0.1, 1,
+                                          np.zeros(2).ctypes.data, None, None) == N.ERR_NO_DEVICE
+
+
+@pytest.mark.skipif(not os.path.isdir(os.path.join(REFERENCE_ROOT, "examples")), reason="reference checkout absent")
+@pytest.mark.parametrize("path,solvers", [("examples/oculomotor.cl", [0, 1, 2, 3, 4]), ("tests/oculomotor.cl", [2, 4]),
+                                          ("examples/kuramoto.cl", [0, 1, 2]), ("tests/kuramoto.cl", [0, 1])])
+def test_reference_system_files_compile_unchanged(path, solvers):
+    """Drop-in: the reference's own system files build as they are."""
+    src = open(os.path.join(REFERENCE_ROOT, path)).read()
+    neq = 6 if "oculomotor" in path else 5
+    for solver in solvers:
+        nnoi = (2 if neq == 6 else neq) if solver == 0 else 0
+        npar = (6 if neq == 6 else neq + 1) + nnoi
+        rc, ctx = _create(solver=solver, num_equat=neq, num_params=npar, num_noi=nnoi)
+        assert rc == N.OK
+        assert _compile(ctx, src) == N.OK, N.last_error(ctx)
+        N.lib.sodecl_cuda_destroy(ctx)
+
+
+def test_python_module_fails_cleanly_without_device():
+    from sodecl_b200 import sodecl_interface
+
+    if N.device_count() > 0:
+        pytest.skip("checks the no-device path")
+    out = sodecl_interface.sodeclcall([0.0], [0, 0, 0, 0, 0, 2.0], [120, 1.5, 0.0045, 0.05, 600, 9.0], 0, 0,
+                                      system_path("oculomotor"), 2, 1, 6, 6, 0, 1e-3, 0.01, 10, 0)
+    assert out == []
+    out = sodecl_interface.sodeclcall([0.0], [0.0] * 6, [1.0] * 6, 0, 0, system_path("oculomotor"), 9, 1, 6, 6, 0,
+                                      1e-3, 0.01, 10, 0)
+    assert out == []

@@ -1,0 +1,330 @@
+"""Parity of the CUDA path with the CPU oracle and the reference's known answers.
+
+Every result goes through libsodecl_cuda.so (C ABI) on cuda:0 and is compared
+with the oracle (oracle/oracle_solvers.h, itself pinned to the reference in
+test_oracle.py) on the same inputs.
+
+Tolerance (FP64): per element, |gpu - oracle| <= RTOL * (|oracle| + 1e-3 * S_e),
+S_e = the largest |value| of equation e in the run (so that values crossing
+zero are measured against their equation's scale), RTOL = 1e-12.  With
+fmad=0 the GPU evaluates in the oracle's exact order, and only the last-bit
+differences of CUDA's exp/log/sin/cos against glibc remain; with fmad=1
+(default) FMA contraction adds rounding differences of the same order.
+Threefry words, u01 doubles and draw counters: bit-exact.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import sodecl_b200
+from sodecl_b200 import _native as N
+from sodecl_b200 import Integrator, system_path
+from oracle.oracle import Oracle, printed_dt, to_reference_layout
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+NOMINAL = np.array([120.0, 1.5, 0.0045, 0.05, 600.0, 9.0])
+Y0 = np.array([0.0, 0.0, 0.0, 0.0, 0.0, 2.0])
+RTOL = 1e-12
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    if N.device_count() < 1:
+        pytest.fail("no CUDA device: the gpu tests need a B200")
+
+
+def rel_error(got, want):
+    """max over elements of |got - want| / (|want| + 1e-3 * scale of that equation)."""
+    got, want = np.asarray(got), np.asarray(want)
+    scale = np.abs(want).max(axis=tuple(i for i in range(want.ndim) if i != 1), keepdims=True)
+    den = np.abs(want) + 1e-3 * scale + 1e-300
+    return float(np.max(np.abs(got - want) / den))
+
+
+def run_gpu(system, solver, t0, y0, p, counters=None, **kw):
+    n = len(t0)
+    with Integrator(system_path(system), solver, orbits=n, **kw) as sim:
+        sim.upload(t0, y0, p, counters)
+        rec = sim.run()
+        t, y, cnt = sim.state()
+        passes, flags = sim.status()
+    return rec, t, y, cnt, passes, flags
+
+
+# --------------------------------------------------------------------------
+# the reference's own known-answer tests, through the drop-in Python API
+
+
+@pytest.mark.parametrize("name,solver,dt,ksteps", [("euler", 1, 1e-8, 40000), ("rk", 2, 1e-6, 400),
+                                                    ("ie", 3, 1e-6, 400), ("im", 4, 1e-6, 400)])
+def test_reference_known_answers_through_sodecl_py(name, solver, dt, ksteps):
+    from sodecl_b200.sodecl import sodecl
+
+    orbits, nequat = 2, 6
+    initx = np.tile(Y0, (orbits, 1))
+    params = np.tile(NOMINAL, (orbits, 1))
+    t, results = sodecl(0, 0, system_path("oculomotor"), initx, params, solver, orbits, nequat, 0, dt, 0.1, ksteps, 0)
+    golden = np.load(os.path.join(GOLDEN, "oculomotor_%s.npy" % name))
+    assert results.shape == golden.shape
+    assert np.isclose(results, golden).all()  # the reference test's rule
+    want = to_reference_layout(Oracle("oculomotor").run(solver, np.zeros(2), initx, params, neq=6, npar=6, dt=dt,
+                                                        tspan=0.1, ksteps=ksteps).records)
+    assert rel_error(results.T, want.T) < RTOL
+
+
+def test_reference_python_module_list_interface():
+    from sodecl_b200 import sodecl_interface
+
+    out = sodecl_interface.sodeclcall([0.0, 0.0], list(np.tile(Y0, 2)), list(np.tile(NOMINAL, 2)), 0, 0,
+                                      system_path("oculomotor"), 2, 2, 6, 6, 0, 1e-6, 0.1, 400, 0)
+    golden = np.load(os.path.join(GOLDEN, "oculomotor_rk.npy"))
+    res = np.array(out).reshape(12, -1, order="F")
+    assert np.isclose(res, golden).all()
+
+
+# --------------------------------------------------------------------------
+# fixtures produced by the reference's kernels compiled as C
+
+
+@pytest.mark.parametrize("fmad", [0, 1])
+@pytest.mark.parametrize("name,system", [("kuramoto_euler", "kuramoto"), ("kuramoto_se", "kuramoto"),
+                                         ("kuramoto32_se", "kuramoto"), ("oculomotor_se", "oculomotor"),
+                                         ("oculomotor_im", "oculomotor"), ("oculomotor_ie", "oculomotor"),
+                                         ("oculomotor_rk4", "oculomotor")])
+def test_reference_build_fixtures(name, system, fmad):
+    f = dict(np.load(os.path.join(GOLDEN, "ref_%s.npz" % name)))
+    n = len(f["t0"])
+    solver = int(f["solver"])
+    kw = dict(dt=float(f["dt"]), tspan=float(f["tspan"]), ksteps=int(f["ksteps"]), neq=int(f["neq"]),
+              npar=int(f["npar"]), nnoi=int(f["nnoi"]), fmad=bool(fmad))
+    if int(f["orbit_offset"]):
+        # the noise stream is keyed by the global orbit index: run the fixture's
+        # orbits as the tail of a larger list
+        off = int(f["orbit_offset"])
+        pad = lambda a: np.concatenate([np.repeat(a[:1], off, axis=0), a])  # noqa: E731
+        rec, t, y, cnt, _, _ = run_gpu(system, solver, pad(f["t0"]), pad(f["y0"]), pad(f["params"]),
+                                       pad(f["counters"]) if "counters" in f else None, **kw)
+        rec, t, y, cnt = rec[:, :, off:], t[off:], y[off:], cnt[off:]
+    else:
+        rec, t, y, cnt, _, _ = run_gpu(system, solver, f["t0"], f["y0"], f["params"], f.get("counters"), **kw)
+    assert rec.shape == f["records"].shape
+    err = rel_error(rec, f["records"])
+    print("%s fmad=%d: max rel error %.3g" % (name, fmad, err))
+    assert err < (RTOL if name != "kuramoto_euler" else 1e-10)
+    np.testing.assert_array_equal(t, f["t_final"])
+    if "counters" in f:
+        np.testing.assert_array_equal(cnt, f["counters_final"])
+
+
+# --------------------------------------------------------------------------
+# oracle parity on random inputs, every solver, both precisions
+
+
+def oculomotor_inputs(n, seed, nnoi=0):
+    rng = np.random.default_rng(seed)
+    p = NOMINAL * rng.uniform(0.5, 1.5, (n, 6))
+    if nnoi:
+        p = np.concatenate([p, rng.uniform(0.0, 0.1, (n, nnoi))], axis=1)
+    return np.zeros(n), np.tile(Y0, (n, 1)), p
+
+
+@pytest.mark.parametrize("fmad", [0, 1])
+@pytest.mark.parametrize("solver,dt", [(1, 1e-6), (2, 1e-5), (3, 1e-3), (4, 1e-3), (0, 1e-5)])
+def test_oculomotor_parity_fp64(solver, dt, fmad):
+    n = 1000  # not a multiple of the block size
+    nnoi = 2 if solver == 0 else 0
+    t0, y0, p = oculomotor_inputs(n, solver, nnoi)
+    cnt = np.arange(n) * 1000.0 if nnoi else None
+    kw = dict(dt=dt, tspan=300 * dt, ksteps=30, neq=6, npar=6 + nnoi, nnoi=nnoi)
+    rec, t, y, c, passes, flags = run_gpu("oculomotor", solver, t0, y0, p, cnt, fmad=bool(fmad), **kw)
+    ref = Oracle("oculomotor").run(solver, t0, y0, p, counters=cnt, **kw)
+    err = rel_error(rec, ref.records)
+    print("solver %d fmad=%d: max rel error %.3g" % (solver, fmad, err))
+    assert err < RTOL
+    np.testing.assert_array_equal(t, ref.t)
+    if solver in (3, 4):
+        if not fmad:
+            # same iterates -> same pass counts
+            assert np.mean(passes == ref.newton_passes) > 0.99
+        assert abs(passes.sum() / ref.newton_passes.sum() - 1) < 1e-3
+        assert not (flags & N.FLAG_NEWTON_CAP).any()
+    if nnoi:
+        np.testing.assert_array_equal(c, ref.counters)
+
+
+@pytest.mark.parametrize("solver,dt", [(1, 1e-6), (2, 1e-5), (3, 1e-4), (4, 1e-4)])
+def test_oculomotor_parity_fp32(solver, dt):
+    n = 512
+    t0, y0, p = oculomotor_inputs(n, 10 + solver)
+    kw = dict(dt=dt, tspan=100 * dt, ksteps=10, neq=6, npar=6)
+    rec, *_ = run_gpu("oculomotor", solver, t0, y0, p, precision="fp32", **kw)
+    ref32 = Oracle("oculomotor", "fp32").run(solver, t0, y0, p, **kw).records
+    ref64 = Oracle("oculomotor", "fp64").run(solver, t0, y0, p, **kw).records
+    e32, e64 = rel_error(rec, ref32), rel_error(rec, ref64)
+    print("fp32 solver %d: vs fp32 oracle %.3g, vs fp64 oracle %.3g" % (solver, e32, e64))
+    assert e32 < 1e-4
+    assert e64 < 1e-3
+
+
+@pytest.mark.parametrize("N_osc,solver,nnoi", [(8, 1, 0), (8, 2, 0), (16, 3, 0), (4, 4, 0), (32, 0, 32), (5, 0, 5)])
+def test_kuramoto_parity(N_osc, solver, nnoi):
+    n = 300
+    rng = np.random.default_rng(N_osc)
+    p = np.concatenate([rng.uniform(0, 5, (n, 1)), np.tile(rng.normal(size=N_osc), (n, 1))] +
+                       ([rng.uniform(0, 0.5, (n, N_osc))] if nnoi else []), axis=1)
+    th0 = rng.uniform(0, 2 * np.pi, (n, N_osc))
+    cnt = rng.integers(0, 2 ** 40, n).astype(float) if nnoi else None
+    kw = dict(dt=0.01, tspan=2.0, ksteps=20, neq=N_osc, npar=p.shape[1], nnoi=nnoi)
+    rec, t, y, c, *_ = run_gpu("kuramoto", solver, np.zeros(n), th0, p, cnt, **kw)
+    ref = Oracle("kuramoto").run(solver, np.zeros(n), th0, p, counters=cnt, **kw)
+    err = rel_error(rec, ref.records)
+    print("kuramoto N=%d solver %d: max rel error %.3g" % (N_osc, solver, err))
+    assert err < 1e-10
+    if nnoi:
+        np.testing.assert_array_equal(c, ref.counters)
+
+
+# --------------------------------------------------------------------------
+# the noise stream, bit for bit
+
+
+def test_noise_stream_bit_exact():
+    o = Oracle("kuramoto")
+    rng = np.random.default_rng(5)
+    gids = np.concatenate([np.arange(8), rng.integers(0, 2 ** 31, 56)])
+    counters = np.concatenate([np.zeros(8), rng.integers(0, 2 ** 52, 48).astype(float), -rng.uniform(0, 1e11, 8)])
+    nnoi, nsteps, dt = 5, 7, 0.01
+    normals, words, u01 = sodecl_b200.noise_stream(gids, counters, nnoi, printed_dt(dt), nsteps, words=True, u01=True)
+    ncalls = (nnoi + 1) // 2
+    for i in range(len(gids)):
+        c = counters[i]
+        for s in range(nsteps):
+            for k in range(ncalls):
+                w = o.threefry2x64_20([int(gids[i]), o.counter_word(c)], [0, 0xF00DCAFE])
+                np.testing.assert_array_equal(words[i, s, k], w)
+                assert u01[i, s, k, 0] == o.u01_open_open(int(w[0]))
+                assert u01[i, s, k, 1] == o.u01_open_open(int(w[1]))
+                c += 1
+        want = o.noise_stream(int(gids[i]), counters[i], nnoi, dt, nsteps)
+        # Box-Muller through CUDA's and glibc's log/sin/cos: a few ulp
+        ulp = np.spacing(np.abs(want))
+        assert np.max(np.abs(normals[i] - want) / ulp) <= 8
+
+
+# --------------------------------------------------------------------------
+# status words, continuation, output modes, scale
+
+
+def test_newton_cap_and_nonfinite_flags():
+    n = 64
+    t0, y0, p = oculomotor_inputs(n, 1)
+    rec, t, y, c, passes, flags = run_gpu("oculomotor", 4, t0, y0, p, dt=1e-3, tspan=0.01, ksteps=10, neq=6, npar=6,
+                                          newton_tol=1e-14, newton_max_iter=3)
+    assert (flags & N.FLAG_NEWTON_CAP).all()
+    assert (passes == 30).all()
+    # RK4 at dt=1e-3 diverges for this model
+    rec, t, y, c, passes, flags = run_gpu("oculomotor", 2, t0, y0, p, dt=1e-3, tspan=2.0, ksteps=100, neq=6, npar=6)
+    bad = ~np.isfinite(rec[-1]).all(axis=0)
+    assert bad.any()
+    np.testing.assert_array_equal((flags & N.FLAG_NONFINITE) != 0, ~np.isfinite(rec).all(axis=(0, 1)))
+
+
+def test_second_run_continues_from_device_state():
+    n = 200
+    t0, y0, p = oculomotor_inputs(n, 2)
+    kw = dict(dt=1e-5, ksteps=20, neq=6, npar=6)
+    with Integrator(system_path("oculomotor"), "rk4", orbits=n, tspan=2e-3, **kw) as sim:
+        sim.upload(t0, y0, p)
+        a = sim.run()
+        b = sim.run()
+    with Integrator(system_path("oculomotor"), "rk4", orbits=n, tspan=4e-3, **kw) as sim:
+        sim.upload(t0, y0, p)
+        whole = sim.run()
+    np.testing.assert_array_equal(b[0], a[-1])
+    np.testing.assert_array_equal(np.concatenate([a, b[1:]]), whole)
+
+
+def test_output_modes_agree():
+    torch = pytest.importorskip("torch")
+    n = 4096
+    t0, y0, p = oculomotor_inputs(n, 3)
+    kw = dict(dt=1e-5, tspan=1e-3, ksteps=10, neq=6, npar=6)
+    outs = []
+    with Integrator(system_path("oculomotor"), "rk4", orbits=n, **kw) as sim:
+        shape = (sim.num_records, 6, n)
+        sim.upload(t0, y0, p)
+        outs.append(sim.run())                                     # pageable host
+        sim.upload(t0, y0, p)
+        pinned = torch.empty(shape, dtype=torch.float64, pin_memory=True)
+        sim.run_into(pinned.data_ptr(), pinned.numel())            # pinned host
+        outs.append(pinned.numpy().copy())
+        sim.upload(t0, y0, p)
+        dev = torch.empty(shape, dtype=torch.float64, device="cuda")
+        sim.run_into(dev.data_ptr(), dev.numel())                  # device
+        torch.cuda.synchronize()
+        outs.append(dev.cpu().numpy())
+        sim.upload(t0, y0, p)
+        assert sim.run(discard=True) is None                       # output_Type::None
+        t_none, y_none, _ = sim.state()
+    for o in outs[1:]:
+        np.testing.assert_array_equal(o, outs[0])
+    np.testing.assert_array_equal(y_none, outs[0][-1].T)
+
+
+def test_device_launch_api_in_chunks():
+    torch = pytest.importorskip("torch")
+    n = 3000
+    t0, y0, p = oculomotor_inputs(n, 4)
+    kw = dict(dt=1e-5, tspan=2e-3, ksteps=20, neq=6, npar=6)
+    with Integrator(system_path("oculomotor"), "rk4", orbits=n, **kw) as sim:
+        sim.upload(t0, y0, p)
+        want = sim.run()
+        nchunks = sim.num_chunks
+        dt_ = torch.tensor(t0, device="cuda")
+        dy = torch.tensor(y0, device="cuda")
+        dp = torch.tensor(p, device="cuda")
+        rec = torch.full((nchunks + 1, 6, n), float("nan"), dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream().cuda_stream
+        # two orbit halves x three interval ranges
+        for lo, hi in ((0, 1000), (1000, n)):
+            for c0, c1 in ((0, 3), (3, 7), (7, nchunks)):
+                sim.launch(t=dt_[lo:].data_ptr(), y=dy[lo:].data_ptr(), params=dp[lo:].data_ptr(),
+                           records=rec.data_ptr(), n=hi - lo, orbit_offset=lo, rec_stride=n, rec_col0=lo,
+                           chunk_begin=c0, chunk_end=c1, write_final=(c1 == nchunks), stream=stream)
+        torch.cuda.synchronize()
+    np.testing.assert_array_equal(rec.cpu().numpy(), want)
+
+
+def test_many_orbits_indexing():
+    n = 1 << 18
+    t0, y0, p = oculomotor_inputs(n, 6)
+    kw = dict(dt=1e-5, tspan=2e-4, ksteps=5, neq=6, npar=6)
+    rec, *_ = run_gpu("oculomotor", 2, t0, y0, p, **kw)
+    idx = np.r_[0:256, n // 2 - 128:n // 2 + 128, n - 256:n]
+    ref = Oracle("oculomotor").run(2, t0[idx], y0[idx], p[idx], **kw).records
+    assert rel_error(rec[:, :, idx], ref) < RTOL
+    assert np.isfinite(rec).all()
+
+
+def test_cpp_sodeclmgr_drop_in(tmp_path):
+    """The C++ manager with the reference's call sequence (interfaces/python/sodecl.cpp:56-94)."""
+    src = os.path.join(REPO, "tests", "cpp", "sodeclmgr_golden.cpp")
+    exe = str(tmp_path / "sodeclmgr_golden")
+    lib_dir = os.path.join(REPO, "sodecl_b200")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", os.path.join(REPO, "include"), src, "-o", exe, "-L", lib_dir,
+                    "-lsodecl_cuda", "-Wl,-rpath," + lib_dir], check=True)
+    out_file = str(tmp_path / "out.bin")
+    proc = subprocess.run([exe, system_path("oculomotor"), out_file], capture_output=True, text=True, cwd=tmp_path)
+    assert proc.returncode == 0, proc.stdout + proc.stderr
+    assert "Compute results runtime" in proc.stdout
+    res = np.fromfile(out_file).reshape(12, -1, order="F")
+    golden = np.load(os.path.join(GOLDEN, "oculomotor_rk.npy"))
+    assert np.isclose(res, golden).all()
+    filemode = np.fromfile(str(tmp_path / "sodecloutput.bin"))
+    np.testing.assert_array_equal(filemode, np.fromfile(out_file))
