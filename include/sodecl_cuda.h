@@ -58,6 +58,14 @@ extern "C" {
 #define SODECL_FP64 0
 #define SODECL_FP32 1
 
+/* how FP64 programs divide: SODECL_DIV_RECIPROCAL computes a/b as a*r plus two
+ * FMA corrections with r = 1/b (hoistable out of the step loop for parameters
+ * and constants), falling back to IEEE division outside [2^-500, 2^500); same
+ * bits as SODECL_DIV_IEEE.  Which is faster depends on the system file (on the
+ * oculomotor RK4 workload IEEE is); sodecl_cuda_autotune measures it. */
+#define SODECL_DIV_RECIPROCAL 0
+#define SODECL_DIV_IEEE 1
+
 /* per-orbit status flags (sodecl_cuda_status) */
 #define SODECL_FLAG_NEWTON_CAP 1   /* some implicit step stopped at newton_max_iter */
 #define SODECL_FLAG_NONFINITE 2    /* a stored record held NaN or Inf */
@@ -84,9 +92,12 @@ typedef struct sodecl_cfg {
     int32_t newton_max_iter; /* implicit solvers' pass limit; default 1000 (ie.cl:69, im.cl:65) */
     int32_t record_f32;      /* device-API records stored as float (sodecl_cuda_launch only) */
     int32_t min_blocks_per_sm; /* launch-bounds occupancy hint for the compiler; 0 = none */
+    int32_t division;        /* FP64 quotients: SODECL_DIV_IEEE (default) or SODECL_DIV_RECIPROCAL;
+                                both give the IEEE-rounded quotient bit for bit */
 } sodecl_cfg;
 
-/* Fills the defaults: Euler, fp64, fmad on, Newton 1e-7 / 1000, device 0. */
+/* Fills the defaults: Euler, fp64, fmad on, Newton 1e-7 / 1000, device 0,
+ * IEEE division. */
 void sodecl_cfg_init(sodecl_cfg *cfg);
 
 /* Validates cfg and makes a context bound to cfg->device.  Needs no GPU
@@ -178,9 +189,101 @@ typedef struct sodecl_launch {
 
 int sodecl_cuda_launch(sodecl_ctx *ctx, const sodecl_launch *launch, void *stream);
 
+/* ---- discrete adjoint (model fitting) -----------------------------------
+ *
+ * For every orbit, the mean squared error of its records against targets,
+ *   loss_i = sum_{r,e} (y_{r,e,i} - target_{r,e,i})^2 / (records * num_equat),
+ * and (optionally) its gradient with respect to the orbit's parameters and
+ * initial state, by the discrete adjoint of the Euler or RK4 steps (FP64):
+ * the user's right-hand side differentiated in reverse mode (the system file
+ * compiled a second time with a recording `double`), the state checkpointed
+ * every `ckpt_every` steps (0: ~sqrt(steps)) and recomputed per segment.
+ * Records, steps and the step size follow the context's configuration; all
+ * pointers are device pointers; the launch goes on `stream`.  No
+ * counterpart in the reference. */
+typedef struct sodecl_adjoint_io {
+    const double *t0;       /* [n] */
+    const double *y0;       /* [n][num_equat] */
+    const double *params;   /* [n][num_params] */
+    const double *targets;  /* [records][num_equat][n] */
+    double *loss;           /* [n] out */
+    double *grad_params;    /* [n][num_params] out, or NULL for the loss alone */
+    double *grad_y0;        /* [n][num_equat] out, or NULL */
+    int32_t *flags;         /* [n] out, or NULL: 4 = tape overflow (raise tape_entries) */
+    int64_t n;              /* orbits, <= list_size */
+    int32_t ckpt_every;     /* steps per checkpoint; 0 = ceil(sqrt(steps)) */
+    int32_t tape_entries;   /* operations one right-hand side may record; 0 = 256 */
+} sodecl_adjoint_io;
+
+#define SODECL_FLAG_TAPE_OVERFLOW 4
+
+int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stream);
+
 /* Kernel resources of the compiled program on its device (registers per
  * thread, local memory bytes per thread, max threads per block).  Needs a GPU. */
 int sodecl_cuda_kernel_info(sodecl_ctx *ctx, int *regs, int *local_bytes, int *max_threads);
+
+/* Autotuner: times candidate launch shapes (threads per block, resident-block
+ * hints) and FP64 division modes on copies of the first `sample_orbits`
+ * uploaded orbits for `sample_steps` steps -- the context's state does not
+ * advance -- and rebuilds the program with the fastest.  All candidates give
+ * identical results.  Writes the choice (any pointer may be NULL). */
+int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_steps, int32_t *block,
+                         int32_t *min_blocks, int32_t *division, double *best_ms);
+
+/* Division mode the program was actually built with (SODECL_DIV_*): the
+ * reciprocal mode falls back to IEEE for system files that need plain double. */
+int sodecl_cuda_program_division(const sodecl_ctx *ctx);
+
+/* ---- heterogeneous batches ----------------------------------------------
+ *
+ * Many orbits of up to 32 classes -- each class a system file with a solver,
+ * sizes and step -- and each orbit with its own step count, integrated by one
+ * persistent kernel that takes orbits from per-class device work queues
+ * (orbits sorted by decreasing step count, lanes refilled as their orbit
+ * finishes), launched through a captured CUDA graph.  Final states only.
+ * No counterpart in the reference, which integrates one system, one solver
+ * and one step count per call (src/sodeclmgr.cpp:921-1035). */
+typedef struct sodecl_batch sodecl_batch;
+
+typedef struct sodecl_class_cfg {
+    int32_t solver;
+    int32_t num_equat;
+    int32_t num_params;
+    int32_t num_noi;
+    double dt;               /* step, printed to 6 significant digits like _m_dt_ */
+    double newton_tol;       /* default 1e-7 */
+    int32_t newton_max_iter; /* default 1000 */
+} sodecl_class_cfg;
+
+void sodecl_class_cfg_init(sodecl_class_cfg *cfg);
+int sodecl_batch_create(int device, int fmad, int division, sodecl_batch **out);
+/* Adds a class (before compile); writes its id. */
+int sodecl_batch_add_class(sodecl_batch *b, const char *system_src, size_t len, const sodecl_class_cfg *cfg,
+                           int32_t *class_id);
+/* Builds one NVRTC program with every class and the persistent kernel. */
+int sodecl_batch_compile(sodecl_batch *b);
+/* n orbits: class, step count, t0; y0 and params packed in orbit order with
+ * each orbit's class widths; counters (NULL unless a class is stochastic). */
+int sodecl_batch_set_items(sodecl_batch *b, int64_t n, const int32_t *item_class, const int64_t *nsteps,
+                           const double *t0, const double *y0, const double *params, const double *counters);
+/* Threads per block (32..256, multiple of 32) and resident blocks per SM
+ * (0 = as many as fit). */
+int sodecl_batch_set_launch(sodecl_batch *b, int32_t block, int32_t blocks_per_sm);
+/* Autotuner: times every candidate launch shape on the current items (each
+ * trial advances them) and keeps the fastest. */
+int sodecl_batch_tune(sodecl_batch *b, int32_t *block, int32_t *blocks_per_sm, double *best_ms);
+/* One persistent launch over every item from its current state; use_graph:
+ * replay a captured CUDA graph (captured on first use). */
+int sodecl_batch_run(sodecl_batch *b, int32_t use_graph);
+/* Final states in the caller's orbit order and packing; any pointer may be NULL. */
+int sodecl_batch_results(sodecl_batch *b, double *t, double *y, double *counters, int64_t *newton_passes,
+                         int32_t *flags);
+int sodecl_batch_last_ms(const sodecl_batch *b, double *ms);
+int sodecl_batch_kernel_info(sodecl_batch *b, int *regs, int *local_bytes);
+size_t sodecl_batch_last_error(const sodecl_batch *b, char *buf, size_t n);
+size_t sodecl_batch_program_source(const sodecl_batch *b, char *buf, size_t n);
+void sodecl_batch_destroy(sodecl_batch *b);
 
 /* ---- test and measurement helpers -------------------------------------- */
 
@@ -193,6 +296,14 @@ int sodecl_cuda_kernel_info(sodecl_ctx *ctx, int *regs, int *local_bytes, int *m
  * Host pointers. */
 int sodecl_cuda_noise_stream(int device, const int64_t *gids, const double *counters, int64_t n, int32_t nnoi,
                              double dt_program, int64_t nsteps, double *normals, uint64_t *words, double *u01);
+
+/* Compares the reciprocal quotient of SODECL_DIV_RECIPROCAL with IEEE
+ * division, bit for bit, on `pairs` pseudo-random operand pairs (every
+ * exponent, significands near 1 and 2, zeros, subnormals, Inf, NaN) drawn
+ * from `seed`.  Writes the number of differing results and the first
+ * differing pair. */
+int sodecl_cuda_division_check(int device, int64_t pairs, uint64_t seed, int64_t *mismatches, double *first_a,
+                               double *first_b);
 
 /* Issue-rate microbenchmark of the FP64 (precision 0) or FP32 (1) FMA pipe:
  * independent FMA chains on every SM, timed with CUDA events.  Writes the

@@ -184,3 +184,34 @@ def to_reference_layout(records: np.ndarray) -> np.ndarray:
     reference's Python wrapper returns (interfaces/python/sodecl.py:80)."""
     nrec = records.shape[0]
     return records.reshape(nrec, -1).T.copy()
+
+
+def reference_gradient(system_file, solver, neq, npar, dt, ksteps, nchunks, t0, y0, params, targets):
+    """(loss[n], grad_params[n,npar], grad_y0[n,neq]) of the per-orbit MSE by
+    forward-mode dual numbers through the system file (oracle/gradient.cpp),
+    stepping with printed_dt(dt)."""
+    import hashlib
+    import subprocess
+    import tempfile
+
+    src = open(system_file, "rb").read()
+    tag = hashlib.sha256(src + open(os.path.join(HERE, "gradient.cpp"), "rb").read()
+                         + ("%d %d" % (neq, npar)).encode()).hexdigest()[:16]
+    exe = os.path.join(BUILD_DIR, "gradient_%s" % tag)
+    if not os.path.exists(exe):
+        os.makedirs(BUILD_DIR, exist_ok=True)
+        subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", '-DSYSTEM_FILE="%s"' % os.path.abspath(system_file),
+                        "-DNUMEQ=%d" % neq, "-DNUMPAR=%d" % npar, os.path.join(HERE, "gradient.cpp"), "-o", exe],
+                       check=True)
+    t0 = np.ascontiguousarray(t0, dtype=np.float64)
+    n = t0.size
+    with tempfile.TemporaryDirectory() as d:
+        fin, fout = os.path.join(d, "in.bin"), os.path.join(d, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(np.array([n, nchunks, ksteps], dtype=np.int64).tobytes())
+            f.write(np.array([printed_dt(dt)], dtype=np.float64).tobytes())
+            for a in (t0, y0, params, targets):
+                f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
+        subprocess.run([exe, str(solver), fin, fout], check=True)
+        out = np.fromfile(fout)
+    return out[:n], out[n:n + n * npar].reshape(n, npar), out[n + n * npar:].reshape(n, neq)

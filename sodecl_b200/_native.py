@@ -24,6 +24,7 @@ ERR_UNSUPPORTED = -9
 
 STOCHASTIC_EULER, EULER, RUNGE_KUTTA, IMPLICIT_EULER, IMPLICIT_MIDPOINT = range(5)
 FP64, FP32 = 0, 1
+DIV_RECIPROCAL, DIV_IEEE = 0, 1
 FLAG_NEWTON_CAP = 1
 FLAG_NONFINITE = 2
 
@@ -46,6 +47,7 @@ class Cfg(C.Structure):
         ("newton_max_iter", C.c_int32),
         ("record_f32", C.c_int32),
         ("min_blocks_per_sm", C.c_int32),
+        ("division", C.c_int32),
     ]
 
 
@@ -69,6 +71,37 @@ class Launch(C.Structure):
     ]
 
 
+class ClassCfg(C.Structure):
+    _fields_ = [
+        ("solver", C.c_int32),
+        ("num_equat", C.c_int32),
+        ("num_params", C.c_int32),
+        ("num_noi", C.c_int32),
+        ("dt", C.c_double),
+        ("newton_tol", C.c_double),
+        ("newton_max_iter", C.c_int32),
+    ]
+
+
+class AdjointIO(C.Structure):
+    _fields_ = [
+        ("t0", C.c_void_p),
+        ("y0", C.c_void_p),
+        ("params", C.c_void_p),
+        ("targets", C.c_void_p),
+        ("loss", C.c_void_p),
+        ("grad_params", C.c_void_p),
+        ("grad_y0", C.c_void_p),
+        ("flags", C.c_void_p),
+        ("n", C.c_int64),
+        ("ckpt_every", C.c_int32),
+        ("tape_entries", C.c_int32),
+    ]
+
+
+FLAG_TAPE_OVERFLOW = 4
+
+_P = C.c_void_p
 # name -> (restype, argtypes); every function include/sodecl_cuda.h declares
 SIGNATURES = {
     "sodecl_cfg_init": (None, [C.POINTER(Cfg)]),
@@ -88,9 +121,29 @@ SIGNATURES = {
     "sodecl_cuda_abi_version": (C.c_int, []),
     "sodecl_cuda_device_count": (C.c_int, [C.POINTER(C.c_int)]),
     "sodecl_cuda_launch": (C.c_int, [C.c_void_p, C.POINTER(Launch), C.c_void_p]),
+    "sodecl_cuda_program_division": (C.c_int, [C.c_void_p]),
+    "sodecl_cuda_adjoint": (C.c_int, [C.c_void_p, C.POINTER(AdjointIO), C.c_void_p]),
+    "sodecl_cuda_autotune": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                       C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "sodecl_cuda_kernel_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "sodecl_cuda_noise_stream": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_double,
                                            C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "sodecl_cuda_division_check": (C.c_int, [C.c_int, C.c_int64, C.c_uint64, C.POINTER(C.c_int64),
+                                             C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "sodecl_class_cfg_init": (None, [C.POINTER(ClassCfg)]),
+    "sodecl_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(_P)]),
+    "sodecl_batch_add_class": (C.c_int, [_P, C.c_char_p, C.c_size_t, C.POINTER(ClassCfg), C.POINTER(C.c_int32)]),
+    "sodecl_batch_compile": (C.c_int, [_P]),
+    "sodecl_batch_set_items": (C.c_int, [_P, C.c_int64, _P, _P, _P, _P, _P, _P]),
+    "sodecl_batch_set_launch": (C.c_int, [_P, C.c_int32, C.c_int32]),
+    "sodecl_batch_tune": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    "sodecl_batch_run": (C.c_int, [_P, C.c_int32]),
+    "sodecl_batch_results": (C.c_int, [_P, _P, _P, _P, _P, _P]),
+    "sodecl_batch_last_ms": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "sodecl_batch_kernel_info": (C.c_int, [_P, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "sodecl_batch_last_error": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
+    "sodecl_batch_program_source": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
+    "sodecl_batch_destroy": (None, [_P]),
     "sodecl_cuda_fma_peak": (C.c_int, [C.c_int, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
 

@@ -3,12 +3,15 @@
 //    NVRTC solver programs embed (device/threefry.cuh), for bit-exactness
 //    tests against the CPU generator;
 //  * an FMA issue-rate microbenchmark, the denominator of the FP64/FP32
-//    "fraction of issue peak" figures.
+//    "fraction of issue peak" figures;
+//  * a check of the reciprocal quotient (device/fastdiv.cuh) against IEEE
+//    division on random and special operands.
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <vector>
 
+#include "device/fastdiv.cuh"
 #include "device/threefry.cuh"
 #include "sodecl_cuda.h"
 
@@ -44,6 +47,60 @@ __global__ void noise_stream_kernel(const long long *gids, const double *counter
             if (2 * c + 1 < nnoi) normals[base + 2 * c + 1] = n1;
         }
     }
+}
+
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long &x)
+{
+    unsigned long long z = (x += 0x9E3779B97F4A7C15ULL);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// An operand: mostly random bit patterns over every exponent, some with the
+// significand near 1 or 2, some special (0, subnormal, Inf, NaN, extremes).
+__device__ __forceinline__ double division_operand(unsigned long long &state)
+{
+    const unsigned long long u = splitmix64(state);
+    const unsigned kind = (unsigned)(u >> 60);
+    unsigned long long bits = splitmix64(state);
+    if (kind < 8) {
+        // exponent within +-600 of 1, where the fast path runs
+        const unsigned long long e = 1023 - 600 + (u % 1200);
+        bits = (bits & 0x800FFFFFFFFFFFFFULL) | (e << 52);
+    } else if (kind < 11) {
+        const unsigned long long e = 1023 - 30 + (u % 60);
+        const unsigned long long k = (u >> 20) & 63;
+        const unsigned long long m = ((u >> 30) & 1) ? k : (0x000FFFFFFFFFFFFFULL - k);
+        bits = (bits & 0x8000000000000000ULL) | (e << 52) | m;
+    } else if (kind < 15) {
+        // anything: full exponent range, subnormals, Inf, NaN
+    } else {
+        const double special[8] = {0.0, -0.0, 1.0 / 0.0, -1.0 / 0.0, 4.9e-324, 2.2250738585072014e-308,
+                                   1.7976931348623157e308, 6.0};
+        return special[u & 7];
+    }
+    return __longlong_as_double((long long)bits);
+}
+
+__global__ void division_check_kernel(unsigned long long seed, long long per_thread, unsigned long long *mismatches,
+                                      double *first)
+{
+    unsigned long long state = seed ^ (0xD1B54A32D192ED03ULL * (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x + 1));
+    unsigned long long bad = 0;
+    for (long long i = 0; i < per_thread; ++i) {
+        const double a = division_operand(state), b = division_operand(state);
+        const double want = a / b, got = sodecl_div_rcp(a, b);
+        const bool same = (__double_as_longlong(want) == __double_as_longlong(got)) || (want != want && got != got);
+        if (!same) {
+            if (atomicAdd(mismatches, 1ULL) == 0) {
+                first[0] = a;
+                first[1] = b;
+            }
+            ++bad;
+        }
+    }
+    (void)bad;
 }
 
 // Eight independent FMA chains per thread, unrolled; every SM full of warps.
@@ -142,6 +199,42 @@ extern "C" int sodecl_cuda_noise_stream(int device, const int64_t *gids, const d
     cudaFree(d_norm);
     cudaFree(d_words);
     cudaFree(d_u01);
+    return rc;
+}
+
+extern "C" int sodecl_cuda_division_check(int device, int64_t pairs, uint64_t seed, int64_t *mismatches,
+                                          double *first_a, double *first_b)
+{
+    if (pairs < 1 || !mismatches) return SODECL_ERR_INVALID_ARG;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) { cudaGetLastError(); return SODECL_ERR_NO_DEVICE; }
+    DeviceGuard guard(device);
+    const int block = 256, blocks = 148 * 8;
+    const long long per_thread = (pairs + (long long)block * blocks - 1) / ((long long)block * blocks);
+    unsigned long long *d_bad = nullptr;
+    double *d_first = nullptr;
+    if (cudaMalloc(&d_bad, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&d_first, 2 * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(d_bad);
+        return SODECL_ERR_OUT_OF_MEMORY;
+    }
+    int rc = SODECL_OK;
+    cudaMemset(d_bad, 0, sizeof(unsigned long long));
+    cudaMemset(d_first, 0, 2 * sizeof(double));
+    division_check_kernel<<<blocks, block>>>(seed, per_thread, d_bad, d_first);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) rc = SODECL_ERR_CUDA;
+    unsigned long long bad = 0;
+    double first[2] = {0.0, 0.0};
+    if (rc == SODECL_OK) {
+        cudaMemcpy(&bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost);
+        cudaMemcpy(first, d_first, sizeof(first), cudaMemcpyDeviceToHost);
+    }
+    cudaFree(d_bad);
+    cudaFree(d_first);
+    *mismatches = (int64_t)bad;
+    if (first_a) *first_a = first[0];
+    if (first_b) *first_b = first[1];
     return rc;
 }
 

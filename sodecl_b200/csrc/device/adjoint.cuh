@@ -1,0 +1,350 @@
+// Discrete adjoint of the explicit solvers (Euler, RK4) for model fitting:
+// d(loss)/d(params, y0) per orbit, loss = mean squared error of the records
+// against target trajectories.
+//
+// Reverse-mode differentiation of the user's right-hand side: the system
+// file is compiled a second time with `double` mapped to sodecl_ad, a value
+// that records every operation (its partial derivatives and operands) on a
+// per-thread tape.  A reverse sweep over the tape gives the vector-Jacobian
+// products v^T df/dy and v^T df/dp exactly (to rounding) for any system file,
+// branches included (the tape follows the branch taken).
+//
+// The integrator steps are differentiated in their discrete form (the
+// adjoint of the arithmetic the forward pass performs, not of the ODE), and
+// the state is checkpointed every `ckpt_every` steps: the backward pass
+// recomputes each segment's states from its checkpoint, then walks the
+// segment's steps in reverse.  Memory per orbit: T/C checkpoints and C
+// segment states (C ~ sqrt(T) balances the two).
+//
+// Part 1 (before the user file): the tape and the sodecl_ad type.
+// Part 2 (SODECL_ADJOINT_KERNEL, after both copies of the user file): the
+// step adjoints and the kernel.
+
+#ifndef SODECL_ADJOINT_TYPES
+#define SODECL_ADJOINT_TYPES
+
+#ifndef SODECL_TAPE_CAP
+#define SODECL_TAPE_CAP 256
+#endif
+
+// One operation: result = g(operand a, operand b); d = dg/da, e = dg/db.
+// Operand -1 means none (a constant).  Leaves have both operands -1.
+struct sodecl_tape {
+    int n;
+    int overflow;
+    short a[SODECL_TAPE_CAP];
+    short b[SODECL_TAPE_CAP];
+    double da[SODECL_TAPE_CAP];
+    double db[SODECL_TAPE_CAP];
+};
+
+__device__ __forceinline__ int sodecl_tape_push(sodecl_tape *t, int a, double da, int b, double db)
+{
+    if (!t) return -1;
+    const int k = t->n;
+    if (k >= SODECL_TAPE_CAP) {
+        t->overflow = 1;
+        return -1;
+    }
+    t->a[k] = (short)a;
+    t->b[k] = (short)b;
+    t->da[k] = da;
+    t->db[k] = db;
+    t->n = k + 1;
+    return k;
+}
+
+struct sodecl_ad {
+    double v;
+    int id;               // tape entry, -1 for a constant
+    sodecl_tape *tp;
+    __device__ __forceinline__ sodecl_ad() : v(0.0), id(-1), tp(nullptr) {}
+    __device__ __forceinline__ sodecl_ad(double x) : v(x), id(-1), tp(nullptr) {}
+    __device__ __forceinline__ sodecl_ad(float x) : v(x), id(-1), tp(nullptr) {}
+    __device__ __forceinline__ sodecl_ad(int x) : v(x), id(-1), tp(nullptr) {}
+    __device__ __forceinline__ sodecl_ad(unsigned x) : v(x), id(-1), tp(nullptr) {}
+    __device__ __forceinline__ sodecl_ad(long x) : v((double)x), id(-1), tp(nullptr) {}
+    __device__ __forceinline__ sodecl_ad(long long x) : v((double)x), id(-1), tp(nullptr) {}
+    __device__ __forceinline__ sodecl_ad(double x, int i, sodecl_tape *t) : v(x), id(i), tp(t) {}
+    __device__ __forceinline__ explicit operator double() const { return v; }
+    __device__ __forceinline__ explicit operator float() const { return (float)v; }
+    __device__ __forceinline__ explicit operator int() const { return (int)v; }
+    __device__ __forceinline__ explicit operator long() const { return (long)v; }
+    __device__ __forceinline__ explicit operator long long() const { return (long long)v; }
+    __device__ __forceinline__ explicit operator bool() const { return v != 0.0; }
+};
+
+__device__ __forceinline__ sodecl_tape *sodecl_ad_tape(const sodecl_ad &a, const sodecl_ad &b)
+{
+    return a.tp ? a.tp : b.tp;
+}
+
+// result of a binary operation with partials da, db
+__device__ __forceinline__ sodecl_ad sodecl_ad_bin(double v, const sodecl_ad &a, double da, const sodecl_ad &b,
+                                                   double db)
+{
+    if (a.id < 0 && b.id < 0) return sodecl_ad(v);
+    sodecl_tape *t = sodecl_ad_tape(a, b);
+    return sodecl_ad(v, sodecl_tape_push(t, a.id, da, b.id, db), t);
+}
+
+__device__ __forceinline__ sodecl_ad sodecl_ad_un(double v, const sodecl_ad &a, double da)
+{
+    if (a.id < 0) return sodecl_ad(v);
+    return sodecl_ad(v, sodecl_tape_push(a.tp, a.id, da, -1, 0.0), a.tp);
+}
+
+__device__ __forceinline__ sodecl_ad operator+(const sodecl_ad &a) { return a; }
+__device__ __forceinline__ sodecl_ad operator-(const sodecl_ad &a) { return sodecl_ad_un(-a.v, a, -1.0); }
+__device__ __forceinline__ sodecl_ad operator+(const sodecl_ad &a, const sodecl_ad &b)
+{
+    return sodecl_ad_bin(a.v + b.v, a, 1.0, b, 1.0);
+}
+__device__ __forceinline__ sodecl_ad operator-(const sodecl_ad &a, const sodecl_ad &b)
+{
+    return sodecl_ad_bin(a.v - b.v, a, 1.0, b, -1.0);
+}
+__device__ __forceinline__ sodecl_ad operator*(const sodecl_ad &a, const sodecl_ad &b)
+{
+    return sodecl_ad_bin(a.v * b.v, a, b.v, b, a.v);
+}
+__device__ __forceinline__ sodecl_ad operator/(const sodecl_ad &a, const sodecl_ad &b)
+{
+    const double q = a.v / b.v;
+    return sodecl_ad_bin(q, a, 1.0 / b.v, b, -q / b.v);
+}
+__device__ __forceinline__ sodecl_ad &operator+=(sodecl_ad &a, const sodecl_ad &b) { return a = a + b; }
+__device__ __forceinline__ sodecl_ad &operator-=(sodecl_ad &a, const sodecl_ad &b) { return a = a - b; }
+__device__ __forceinline__ sodecl_ad &operator*=(sodecl_ad &a, const sodecl_ad &b) { return a = a * b; }
+__device__ __forceinline__ sodecl_ad &operator/=(sodecl_ad &a, const sodecl_ad &b) { return a = a / b; }
+__device__ __forceinline__ bool operator<(const sodecl_ad &a, const sodecl_ad &b) { return a.v < b.v; }
+__device__ __forceinline__ bool operator>(const sodecl_ad &a, const sodecl_ad &b) { return a.v > b.v; }
+__device__ __forceinline__ bool operator<=(const sodecl_ad &a, const sodecl_ad &b) { return a.v <= b.v; }
+__device__ __forceinline__ bool operator>=(const sodecl_ad &a, const sodecl_ad &b) { return a.v >= b.v; }
+__device__ __forceinline__ bool operator==(const sodecl_ad &a, const sodecl_ad &b) { return a.v == b.v; }
+__device__ __forceinline__ bool operator!=(const sodecl_ad &a, const sodecl_ad &b) { return a.v != b.v; }
+
+// elementary functions with their derivatives
+__device__ __forceinline__ sodecl_ad exp(const sodecl_ad &a) { const double e = ::exp(a.v); return sodecl_ad_un(e, a, e); }
+__device__ __forceinline__ sodecl_ad log(const sodecl_ad &a) { return sodecl_ad_un(::log(a.v), a, 1.0 / a.v); }
+__device__ __forceinline__ sodecl_ad sqrt(const sodecl_ad &a) { const double s = ::sqrt(a.v); return sodecl_ad_un(s, a, 0.5 / s); }
+__device__ __forceinline__ sodecl_ad sin(const sodecl_ad &a) { return sodecl_ad_un(::sin(a.v), a, ::cos(a.v)); }
+__device__ __forceinline__ sodecl_ad cos(const sodecl_ad &a) { return sodecl_ad_un(::cos(a.v), a, -::sin(a.v)); }
+__device__ __forceinline__ sodecl_ad tan(const sodecl_ad &a) { const double c = ::cos(a.v); return sodecl_ad_un(::tan(a.v), a, 1.0 / (c * c)); }
+__device__ __forceinline__ sodecl_ad tanh(const sodecl_ad &a) { const double h = ::tanh(a.v); return sodecl_ad_un(h, a, 1.0 - h * h); }
+__device__ __forceinline__ sodecl_ad sinh(const sodecl_ad &a) { return sodecl_ad_un(::sinh(a.v), a, ::cosh(a.v)); }
+__device__ __forceinline__ sodecl_ad cosh(const sodecl_ad &a) { return sodecl_ad_un(::cosh(a.v), a, ::sinh(a.v)); }
+__device__ __forceinline__ sodecl_ad atan(const sodecl_ad &a) { return sodecl_ad_un(::atan(a.v), a, 1.0 / (1.0 + a.v * a.v)); }
+__device__ __forceinline__ sodecl_ad exp2(const sodecl_ad &a) { const double e = ::exp2(a.v); return sodecl_ad_un(e, a, e * 0.6931471805599453); }
+__device__ __forceinline__ sodecl_ad log10(const sodecl_ad &a) { return sodecl_ad_un(::log10(a.v), a, 0.4342944819032518 / a.v); }
+__device__ __forceinline__ sodecl_ad fabs(const sodecl_ad &a) { return sodecl_ad_un(::fabs(a.v), a, a.v < 0.0 ? -1.0 : 1.0); }
+__device__ __forceinline__ sodecl_ad pow(const sodecl_ad &a, const sodecl_ad &b)
+{
+    const double r = ::pow(a.v, b.v);
+    const double da = (b.v == 0.0) ? 0.0 : b.v * ::pow(a.v, b.v - 1.0);
+    const double db = (a.v > 0.0) ? r * ::log(a.v) : 0.0;
+    return sodecl_ad_bin(r, a, da, b, db);
+}
+__device__ __forceinline__ sodecl_ad fmin(const sodecl_ad &a, const sodecl_ad &b) { return a.v <= b.v ? a : b; }
+__device__ __forceinline__ sodecl_ad fmax(const sodecl_ad &a, const sodecl_ad &b) { return a.v >= b.v ? a : b; }
+__device__ __forceinline__ bool isfinite(const sodecl_ad &a) { return ::isfinite(a.v); }
+__device__ __forceinline__ bool isnan(const sodecl_ad &a) { return ::isnan(a.v); }
+
+// reverse sweep: adj[k] holds d(output . seed)/d(entry k) on return
+__device__ __forceinline__ void sodecl_tape_sweep(const sodecl_tape &t, double *adj)
+{
+    for (int k = t.n - 1; k >= 0; --k) {
+        const double g = adj[k];
+        if (g == 0.0) continue;
+        const int a = t.a[k], b = t.b[k];
+        if (a >= 0) adj[a] += t.da[k] * g;
+        if (b >= 0) adj[b] += t.db[k] * g;
+    }
+}
+#endif  // SODECL_ADJOINT_TYPES
+
+#ifdef SODECL_ADJOINT_KERNEL
+// ---------------------------------------------------------------------------
+// Part 2.  Needs: the plain system (sode_system), the recording copy
+// (sodecl_adsys::sode_system), the solver step functions (solvers.cuh).
+
+// f(t, x) and, for the seed v, xbar += v^T df/dx, pbar += v^T df/dp.
+__device__ __forceinline__ void sodecl_vjp(double t, const double *x, const double *p, const double *v, double *xbar,
+                                           double *pbar, sodecl_tape &tape, double *adj, int &overflow)
+{
+    tape.n = 0;
+    tape.overflow = 0;
+    sodecl_ad xa[_numeq_], pa[SODECL_NPAR_ALLOC], fa[_numeq_];
+    for (int e = 0; e < _numeq_; ++e) xa[e] = sodecl_ad(x[e], sodecl_tape_push(&tape, -1, 0.0, -1, 0.0), &tape);
+    for (int j = 0; j < _numpar_; ++j) pa[j] = sodecl_ad(p[j], sodecl_tape_push(&tape, -1, 0.0, -1, 0.0), &tape);
+    sodecl_adsys::sode_system(sodecl_ad(t), xa, fa, pa);
+    for (int k = 0; k < tape.n; ++k) adj[k] = 0.0;
+    for (int e = 0; e < _numeq_; ++e)
+        if (fa[e].id >= 0) adj[fa[e].id] += v[e];
+    sodecl_tape_sweep(tape, adj);
+    for (int e = 0; e < _numeq_; ++e) xbar[e] += adj[e];
+    for (int j = 0; j < _numpar_; ++j) pbar[j] += adj[_numeq_ + j];
+    if (tape.overflow) overflow = 1;
+}
+
+// lambda <- (d step / d y)^T lambda, pbar += (d step / d p)^T lambda, for the
+// step taken from (t, y) with step h: the adjoint of sodecl_step_euler /
+// sodecl_step_rk4's arithmetic.
+__device__ __forceinline__ void sodecl_step_adjoint(double h, double t, const double *y, const double *p,
+                                                    double *lambda, double *pbar, sodecl_tape &tape, double *adj,
+                                                    int &overflow)
+{
+#if SODECL_SOLVER == 1
+    // y1 = y + h f(t, y)
+    double seed[_numeq_], ybar[_numeq_];
+    for (int e = 0; e < _numeq_; ++e) {
+        seed[e] = h * lambda[e];
+        ybar[e] = lambda[e];
+    }
+    sodecl_vjp(t, y, p, seed, ybar, pbar, tape, adj, overflow);
+    for (int e = 0; e < _numeq_; ++e) lambda[e] = ybar[e];
+#elif SODECL_SOLVER == 2
+    // y1 = y + (k1 + 2 k2 + 2 k3 + k4) h / 6 with stage inputs
+    // x1 = y, x2 = y + (h/2) k1, x3 = y + (h/2) k2, x4 = y + h k3
+    double k[_numeq_], x2[_numeq_], x3[_numeq_], x4[_numeq_];
+    double pv[SODECL_NPAR_ALLOC];
+    for (int j = 0; j < _numpar_; ++j) pv[j] = p[j];
+    {
+        real_t yy[_numeq_], kk[_numeq_], pp[SODECL_NPAR_ALLOC], xx[_numeq_];
+        for (int e = 0; e < _numeq_; ++e) yy[e] = (real_t)y[e];
+        for (int j = 0; j < _numpar_; ++j) pp[j] = (real_t)pv[j];
+        sode_system((real_t)t, yy, kk, pp);
+        for (int e = 0; e < _numeq_; ++e) { k[e] = (double)kk[e]; xx[e] = yy[e] + ((real_t)h * (real_t)0.50) * kk[e]; x2[e] = (double)xx[e]; }
+        sode_system((real_t)t + (real_t)0.50 * (real_t)h, xx, kk, pp);
+        for (int e = 0; e < _numeq_; ++e) { xx[e] = yy[e] + ((real_t)h * (real_t)0.50) * kk[e]; x3[e] = (double)xx[e]; }
+        sode_system((real_t)t + (real_t)0.50 * (real_t)h, xx, kk, pp);
+        for (int e = 0; e < _numeq_; ++e) { xx[e] = yy[e] + (real_t)h * kk[e]; x4[e] = (double)xx[e]; }
+        (void)k;
+    }
+    double ybar[_numeq_], kbar[_numeq_], seed[_numeq_], xbar[_numeq_];
+    const double w1 = h / 6.0, w2 = 2.0 * h / 6.0;
+    for (int e = 0; e < _numeq_; ++e) ybar[e] = lambda[e];
+    // stage 4: k4 = f(t + h, x4), weight h/6; x4 depends on y and k3 (factor h)
+    for (int e = 0; e < _numeq_; ++e) { seed[e] = w1 * lambda[e]; xbar[e] = 0.0; }
+    sodecl_vjp(t + h, x4, pv, seed, xbar, pbar, tape, adj, overflow);
+    for (int e = 0; e < _numeq_; ++e) { ybar[e] += xbar[e]; kbar[e] = w2 * lambda[e] + h * xbar[e]; }
+    // stage 3: k3 = f(t + h/2, x3); x3 = y + (h/2) k2
+    for (int e = 0; e < _numeq_; ++e) xbar[e] = 0.0;
+    sodecl_vjp(t + 0.5 * h, x3, pv, kbar, xbar, pbar, tape, adj, overflow);
+    for (int e = 0; e < _numeq_; ++e) { ybar[e] += xbar[e]; kbar[e] = w2 * lambda[e] + 0.5 * h * xbar[e]; }
+    // stage 2: k2 = f(t + h/2, x2); x2 = y + (h/2) k1
+    for (int e = 0; e < _numeq_; ++e) xbar[e] = 0.0;
+    sodecl_vjp(t + 0.5 * h, x2, pv, kbar, xbar, pbar, tape, adj, overflow);
+    for (int e = 0; e < _numeq_; ++e) { ybar[e] += xbar[e]; kbar[e] = w1 * lambda[e] + 0.5 * h * xbar[e]; }
+    // stage 1: k1 = f(t, y)
+    for (int e = 0; e < _numeq_; ++e) xbar[e] = 0.0;
+    sodecl_vjp(t, y, pv, kbar, xbar, pbar, tape, adj, overflow);
+    for (int e = 0; e < _numeq_; ++e) lambda[e] = ybar[e] + xbar[e];
+#else
+#error "the adjoint covers the Euler and RK4 solvers"
+#endif
+}
+
+#define SODECL_FLAG_TAPE_OVERFLOW 4
+
+struct sodecl_adjoint_args {
+    const double *t0;         // [n]
+    const double *y0;         // [n][neq]
+    const double *p;          // [n][npar]
+    const double *targets;    // [nrec][neq][n]
+    double *loss;             // [n] per-orbit mean squared error
+    double *grad_p;           // [n][npar] or null (forward only)
+    double *grad_y0;          // [n][neq] or null
+    double *ckpt;             // scratch [nckpt][neq][n]
+    double *ckpt_t;           // scratch [nckpt][n]
+    double *seg;              // scratch [ckpt_every][neq][n]
+    double *seg_t;            // scratch [ckpt_every][n]
+    int *flags;               // [n] or null
+    long long n;
+    int nchunks;              // records - 1; steps = nchunks * _numsteps_
+    int ckpt_every;           // C
+};
+
+// Loss and, if grad_p is set, its gradient for every orbit.
+extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX) sodecl_adjoint(const sodecl_adjoint_args a)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const long long n = a.n;
+    const int steps = a.nchunks * _numsteps_;
+    const int C = a.ckpt_every;
+    const double w = 1.0 / ((double)(a.nchunks + 1) * _numeq_);  // mean over records x equations
+
+    real_t y[_numeq_], p[SODECL_NPAR_ALLOC];
+    real_t t = (real_t)a.t0[i];
+    for (int e = 0; e < _numeq_; ++e) y[e] = (real_t)a.y0[i * _numeq_ + e];
+    for (int j = 0; j < _numpar_; ++j) p[j] = (real_t)a.p[i * _numpar_ + j];
+    double counter = 0.0;
+    sodecl_i64 passes = 0;
+    int capped = 0;
+
+    // forward: loss at every record, checkpoints every C steps
+    double loss = 0.0;
+    for (int s = 0; s <= steps; ++s) {
+        if (s % _numsteps_ == 0) {
+            const int r = s / _numsteps_;
+            for (int e = 0; e < _numeq_; ++e) {
+                const double d = (double)y[e] - a.targets[((long long)r * _numeq_ + e) * n + i];
+                loss += d * d;
+            }
+        }
+        if (a.grad_p && s % C == 0 && s < steps) {
+            const long long c = s / C;
+            a.ckpt_t[c * n + i] = (double)t;
+            for (int e = 0; e < _numeq_; ++e) a.ckpt[(c * _numeq_ + e) * n + i] = (double)y[e];
+        }
+        if (s < steps) sodecl_advance(t, y, p, i, counter, passes, capped);
+    }
+    a.loss[i] = loss * w;
+    if (!a.grad_p) return;
+
+    // backward, segment by segment from the last
+    sodecl_tape tape;
+    double adj[SODECL_TAPE_CAP];
+    double lambda[_numeq_], pbar[SODECL_NPAR_ALLOC], pd[SODECL_NPAR_ALLOC];
+    for (int e = 0; e < _numeq_; ++e) lambda[e] = 0.0;
+    for (int j = 0; j < _numpar_; ++j) { pbar[j] = 0.0; pd[j] = (double)p[j]; }
+    int overflow = 0;
+    double ynext[_numeq_];  // state after the step being reversed
+    for (int e = 0; e < _numeq_; ++e) ynext[e] = (double)y[e];
+    const int nseg = (steps + C - 1) / C;
+    for (int sg = nseg - 1; sg >= 0; --sg) {
+        const int s0 = sg * C, s1 = min(steps, s0 + C);
+        // recompute the segment's states from its checkpoint
+        real_t ys[_numeq_];
+        real_t ts = (real_t)a.ckpt_t[(long long)sg * n + i];
+        for (int e = 0; e < _numeq_; ++e) ys[e] = (real_t)a.ckpt[((long long)sg * _numeq_ + e) * n + i];
+        for (int s = s0; s < s1; ++s) {
+            const long long c = s - s0;
+            a.seg_t[c * n + i] = (double)ts;
+            for (int e = 0; e < _numeq_; ++e) a.seg[(c * _numeq_ + e) * n + i] = (double)ys[e];
+            sodecl_advance(ts, ys, p, i, counter, passes, capped);
+        }
+        // reverse the segment's steps
+        for (int s = s1 - 1; s >= s0; --s) {
+            // record at state s+1
+            if ((s + 1) % _numsteps_ == 0) {
+                const int r = (s + 1) / _numsteps_;
+                for (int e = 0; e < _numeq_; ++e)
+                    lambda[e] += 2.0 * w * (ynext[e] - a.targets[((long long)r * _numeq_ + e) * n + i]);
+            }
+            const long long c = s - s0;
+            double ystep[_numeq_];
+            for (int e = 0; e < _numeq_; ++e) ystep[e] = a.seg[(c * _numeq_ + e) * n + i];
+            sodecl_step_adjoint((double)_m_dt_, a.seg_t[c * n + i], ystep, pd, lambda, pbar, tape, adj, overflow);
+            for (int e = 0; e < _numeq_; ++e) ynext[e] = ystep[e];
+        }
+    }
+    // record 0 is the initial state
+    for (int e = 0; e < _numeq_; ++e) lambda[e] += 2.0 * w * (ynext[e] - a.targets[(long long)e * n + i]);
+    for (int j = 0; j < _numpar_; ++j) a.grad_p[i * _numpar_ + j] = pbar[j];
+    if (a.grad_y0)
+        for (int e = 0; e < _numeq_; ++e) a.grad_y0[i * _numeq_ + e] = lambda[e];
+    if (a.flags) a.flags[i] = overflow ? SODECL_FLAG_TAPE_OVERFLOW : 0;
+}
+#endif  // SODECL_ADJOINT_KERNEL

@@ -1,0 +1,32 @@
+// Exact division through a reciprocal.  Shared, as text, by the NVRTC
+// programs (embedded by the build) and the statically compiled test kernel in
+// aux_kernels.cu.  Self-contained: no includes.
+#ifndef SODECL_FASTDIV_CUH
+#define SODECL_FASTDIV_CUH
+
+// ---------------------------------------------------------------------------
+// q = a*r, e = fma(-q, b, a), q' = fma(e, r, q) with r = RN(1/b) gives the
+// correctly rounded a/b (Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990): r is
+// within half an ulp of 1/b, q within one ulp of a/b, and the FMA residual
+// is exact as long as nothing under- or overflows -- guaranteed here by
+// requiring |a| and |b| in [2^-500, 2^500); anything else takes the IEEE
+// division.  The point: r = 1/b is a plain division of loop-invariant
+// operands whenever the divisor is a parameter or a constant, so the
+// compiler hoists it out of the step loop and each quotient costs one
+// multiply and two FMAs instead of a full division.  Results are bit-for-bit
+// those of IEEE division.
+__device__ __forceinline__ double sodecl_div_rcp(double a, double b)
+{
+    const double r = 1.0 / b;
+    const double q = a * r;
+    const double e = __fma_rn(-q, b, a);
+    const double q2 = __fma_rn(e, r, q);
+    const unsigned ea = ((unsigned)__double2hiint(a) >> 20) & 0x7ffu;
+    const unsigned eb = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
+    if ((ea - 523u) < 1000u && (eb - 523u) < 1000u)
+        return q2;
+    return a / b;
+}
+
+#endif

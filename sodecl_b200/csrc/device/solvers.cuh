@@ -15,6 +15,7 @@
 //   SODECL_SOLVER        0 Euler-Maruyama, 1 Euler, 2 RK4, 3 implicit Euler,
 //                        4 implicit midpoint (solver_Type numbering)
 //   SODECL_FP32          compute in float
+//   SODECL_FAST_DIV      FP64 through sodecl_f64 (exact reciprocal quotients)
 //   SODECL_RECORD_F32    store records as float (else double)
 //   SODECL_HAS_JACOBIAN  the system file defines calc_jacobian
 //   SODECL_HAS_STOCH     the system file defines sode_system_stoch
@@ -31,12 +32,30 @@ typedef float sodecl_record_t;
 typedef double sodecl_record_t;
 #endif
 
+// IEEE quotient in every build, for divisors that change at every use (the
+// banded solve's pivots), where a reciprocal could not be hoisted.
+__device__ __forceinline__ double sodecl_qdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float sodecl_qdiv(float a, float b) { return a / b; }
+#if SODECL_FAST_DIV
+__device__ __forceinline__ sodecl_f64 sodecl_qdiv(sodecl_f64 a, sodecl_f64 b) { return sodecl_f64(a.v / b.v); }
+#endif
+
+// Loops over equations unroll fully up to 16 equations (state, stages and
+// the Jacobian's bands then live in registers); wider systems keep their
+// arrays in local memory anyway, and full unrolling would only inflate the
+// program, so they unroll by 4.
+#undef SODECL_EQ_UNROLL
+#define SODECL_EQ_UNROLL ((_numeq_) <= 16 ? (_numeq_) : 4)
+#undef SODECL_PAR_UNROLL
+#define SODECL_PAR_UNROLL ((_numpar_) < 1 ? 1 : ((_numpar_) <= 32 ? (_numpar_) : 4))
+
 #define SODECL_NPAR_ALLOC ((_numpar_) > 0 ? (_numpar_) : 1)
 #define SODECL_NNOI_ALLOC ((_numnoi_) > 0 ? (_numnoi_) : 1)
 
 #define SODECL_FLAG_NEWTON_CAP 1
 #define SODECL_FLAG_NONFINITE 2
 
+#ifndef SODECL_STEPS_ONLY
 struct sodecl_args {
     double *t;                  // [n] time of each orbit, in/out
     double *y;                  // [n][_numeq_] state, in/out
@@ -54,13 +73,14 @@ struct sodecl_args {
     sodecl_i64 *newton_passes;  // [n] accumulated Newton passes, or null
     int *flags;                 // [n] or-ed status flags, or null
 };
+#endif
 
 // ---------------------------------------------------------------------------
 // Explicit Euler: y1 = y0 + f(t, y0) h            (src/kernels/euler.cl:10-18)
 __device__ __forceinline__ void sodecl_step_euler(real_t h, real_t t, real_t *y, real_t *ynew, real_t *p)
 {
     sode_system(t, y, ynew, p);
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e)
         ynew[e] = y[e] + ynew[e] * h;
 }
@@ -72,25 +92,25 @@ __device__ __forceinline__ void sodecl_step_rk4(real_t h, real_t t, real_t *y, r
 {
     real_t stage[_numeq_], probe[_numeq_];
     sode_system(t, y, ynew, p);
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) {
         stage[e] = ynew[e];
         probe[e] = y[e] + (h * (real_t)0.50) * stage[e];
     }
     sode_system(t + (real_t)0.50 * h, probe, stage, p);
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) {
         ynew[e] = ynew[e] + (real_t)2.00 * stage[e];
         probe[e] = y[e] + (h * (real_t)0.50) * stage[e];
     }
     sode_system(t + (real_t)0.50 * h, probe, stage, p);
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) {
         ynew[e] = ynew[e] + (real_t)2.00 * stage[e];
         probe[e] = y[e] + h * stage[e];
     }
     sode_system(t + h, probe, stage, p);
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e)
         ynew[e] = y[e] + (ynew[e] + stage[e]) * h / (real_t)6.00;
 }
@@ -108,22 +128,22 @@ __device__ __forceinline__ void sodecl_step_rk4(real_t h, real_t t, real_t *y, r
 __device__ __forceinline__ void sodecl_band_solve(real_t (*m)[_numeq_], real_t *v, real_t *x)
 {
     real_t up[_numeq_], lo[_numeq_], d[_numeq_];
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int i = 0; i < _numeq_; ++i) {
         up[i] = (i < _numeq_ - 2) ? m[i][(i + 1) % _numeq_] : (real_t)0;
         lo[i] = (i < _numeq_ - 1) ? m[(i + 1) % _numeq_][i] : (real_t)0;
         d[i] = m[i][i];
     }
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int i = 1; i < _numeq_; ++i) {
-        const real_t f = up[i] / d[i - 1];
+        const real_t f = sodecl_qdiv(up[i], d[i - 1]);
         d[i] = d[i] - f * lo[i - 1];
         v[i] = v[i] - f * v[i - 1];
     }
-    x[_numeq_ - 1] = v[_numeq_ - 1] / d[_numeq_ - 1];
-#pragma unroll
+    x[_numeq_ - 1] = sodecl_qdiv(v[_numeq_ - 1], d[_numeq_ - 1]);
+#pragma unroll SODECL_EQ_UNROLL
     for (int i = _numeq_ - 2; i >= 0; --i)
-        x[i] = (v[i] - lo[i] * x[i + 1]) / d[i];
+        x[i] = sodecl_qdiv(v[i] - lo[i] * x[i + 1], d[i]);
 }
 
 // Implicit Euler (src/kernels/ie.cl:50-117) and implicit midpoint
@@ -136,7 +156,7 @@ __device__ __forceinline__ int sodecl_step_newton(real_t h, real_t t, real_t *y,
 {
     real_t x[_numeq_], f[_numeq_], r[_numeq_], dx[_numeq_];
     real_t m[_numeq_][_numeq_];
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) x[e] = y[e];
     int pass = 0;
     bool done = false;
@@ -144,14 +164,14 @@ __device__ __forceinline__ int sodecl_step_newton(real_t h, real_t t, real_t *y,
     for (pass = 0; pass < SODECL_NEWTON_MAX; ++pass) {
 #if SODECL_SOLVER == 4
         real_t mid[_numeq_];
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
         for (int e = 0; e < _numeq_; ++e) mid[e] = (y[e] + x[e]) * (real_t)0.5;
         sode_system(t, mid, f, p);
 #else
         sode_system(t, x, f, p);
 #endif
         real_t norm = 0;
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
         for (int e = 0; e < _numeq_; ++e) {
             r[e] = x[e] - y[e] - f[e] * h;
 #if SODECL_SOLVER == 4
@@ -169,18 +189,18 @@ __device__ __forceinline__ int sodecl_step_newton(real_t h, real_t t, real_t *y,
         calc_jacobian(x, m, p);
         const real_t scale = (real_t)(-1.00);
 #endif
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
         for (int i = 0; i < _numeq_; ++i) {
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
             for (int j = 0; j < _numeq_; ++j) m[i][j] = m[i][j] * scale * h;
             m[i][i] = m[i][i] + 1;
         }
         sodecl_band_solve(m, r, dx);
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
         for (int e = 0; e < _numeq_; ++e) x[e] = x[e] - dx[e];
     }
     if (!done) capped = 1;
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) ynew[e] = x[e];
     return done ? pass + 1 : pass;
 }
@@ -196,7 +216,7 @@ __device__ __forceinline__ int sodecl_step_newton(real_t h, real_t t, real_t *y,
 // partner dropped for an odd count.  (stochastic_solver_caller.cl:31-66)
 __device__ __forceinline__ void sodecl_draw_noise(sodecl_i64 gid, double &counter, real_t sqrt_h, real_t *noise)
 {
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int c = 0; c < (_numnoi_ + 1) / 2; ++c) {
         sodecl_u64 w0, w1;
         sodecl_threefry2x64_20((sodecl_u64)gid, sodecl_counter_word(counter), SODECL_TF_KEY0, SODECL_TF_KEY1, w0, w1);
@@ -215,17 +235,41 @@ __device__ __forceinline__ void sodecl_step_em(real_t h, real_t t, real_t *y, re
     real_t g[_numeq_];
     sode_system(t, y, ynew, p);
     sode_system_stoch(t, y, g, p, noise);
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e)
         ynew[e] = y[e] + ynew[e] * h + g[e];
 }
 #endif
 
+// One step of the configured solver from (t, y): y <- y(t + h), t <- t + h,
+// with t advanced as the reference's callers advance it
+// (solver_caller.cl:38, stochastic_solver_caller.cl:71).
+__device__ __forceinline__ void sodecl_advance(real_t &t, real_t *y, real_t *p, sodecl_i64 gid, double &counter,
+                                               sodecl_i64 &passes, int &capped)
+{
+    real_t ynew[_numeq_];
+#if SODECL_SOLVER == 1
+    sodecl_step_euler(_m_dt_, t, y, ynew, p);
+#elif SODECL_SOLVER == 2
+    sodecl_step_rk4(_m_dt_, t, y, ynew, p);
+#elif SODECL_SOLVER == 3 || SODECL_SOLVER == 4
+    passes += sodecl_step_newton(_m_dt_, t, y, ynew, p, capped);
+#elif SODECL_SOLVER == 0
+    real_t noise[SODECL_NNOI_ALLOC];
+    sodecl_draw_noise(gid, counter, sqrt((real_t)_m_dt_), noise);
+    sodecl_step_em(_m_dt_, t, y, ynew, p, noise);
+#endif
+    t = t + _m_dt_;
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) y[e] = ynew[e];
+}
+
+#ifndef SODECL_STEPS_ONLY
 __device__ __forceinline__ void sodecl_store_record(const sodecl_args &a, int rec, sodecl_i64 i, const real_t *y, int &flags)
 {
     sodecl_record_t *row = a.records + (sodecl_i64)(rec - a.rec_first) * _numeq_ * a.rec_stride + a.rec_col0 + i;
     bool finite = true;
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) {
         finite = finite && isfinite(y[e]);
         __stcs(row + (sodecl_i64)e * a.rec_stride, (sodecl_record_t)y[e]);
@@ -240,21 +284,21 @@ sodecl_orbits(const sodecl_args a)
     if (i >= a.n)
         return;
 
-    real_t y[_numeq_], ynew[_numeq_];
+    real_t y[_numeq_];
     real_t p[SODECL_NPAR_ALLOC];
     real_t t = (real_t)a.t[i];
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) y[e] = (real_t)a.y[i * _numeq_ + e];
-#pragma unroll
+#pragma unroll SODECL_PAR_UNROLL
     for (int k = 0; k < _numpar_; ++k) p[k] = (real_t)__ldg(a.p + i * _numpar_ + k);
 
     int flags = 0, capped = 0;
     sodecl_i64 passes = 0;
+    const sodecl_i64 gid = a.orbit_offset + i;
 #if SODECL_SOLVER == 0
     double counter = a.counters[i];
-    real_t noise[SODECL_NNOI_ALLOC];
-    const real_t sqrt_h = sqrt((real_t)_m_dt_);
-    const sodecl_i64 gid = a.orbit_offset + i;
+#else
+    double counter = 0.0;
 #endif
 
 #pragma unroll 1
@@ -262,27 +306,14 @@ sodecl_orbits(const sodecl_args a)
         if (a.records)
             sodecl_store_record(a, c, i, y, flags);
 #pragma unroll 1
-        for (int s = 0; s < _numsteps_; ++s) {
-#if SODECL_SOLVER == 1
-            sodecl_step_euler(_m_dt_, t, y, ynew, p);
-#elif SODECL_SOLVER == 2
-            sodecl_step_rk4(_m_dt_, t, y, ynew, p);
-#elif SODECL_SOLVER == 3 || SODECL_SOLVER == 4
-            passes += sodecl_step_newton(_m_dt_, t, y, ynew, p, capped);
-#elif SODECL_SOLVER == 0
-            sodecl_draw_noise(gid, counter, sqrt_h, noise);
-            sodecl_step_em(_m_dt_, t, y, ynew, p, noise);
-#endif
-            t = t + _m_dt_;
-#pragma unroll
-            for (int e = 0; e < _numeq_; ++e) y[e] = ynew[e];
-        }
+        for (int s = 0; s < _numsteps_; ++s)
+            sodecl_advance(t, y, p, gid, counter, passes, capped);
     }
     if (a.write_final && a.records)
         sodecl_store_record(a, a.chunk_end, i, y, flags);
 
     a.t[i] = (double)t;
-#pragma unroll
+#pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) a.y[i * _numeq_ + e] = (double)y[e];
 #if SODECL_SOLVER == 0
     a.counters[i] = counter;
@@ -291,3 +322,4 @@ sodecl_orbits(const sodecl_args a)
     if (a.newton_passes) a.newton_passes[i] += passes;
     if (a.flags && flags) a.flags[i] |= flags;
 }
+#endif  // SODECL_STEPS_ONLY

@@ -11,8 +11,15 @@
 
 #include <nvrtc.h>
 
+#include <dlfcn.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <cctype>
+#include <cstdint>
+#include <cstdio>
 #include <cstdlib>
+#include <fstream>
 #include <mutex>
 #include <regex>
 #include <sstream>
@@ -22,7 +29,7 @@
 namespace sodecl_b200 {
 
 namespace {
-#include "embedded_sources.inc"  // kPreludeSrc, kThreefrySrc, kSolversSrc (generated by build.py)
+#include "embedded_sources.inc"  // kFastDivSrc kPreludeSrc kThreefrySrc kSolversSrc kBatchSrc kAdjointSrc (build.py)
 
 // Splits `src` into code / comment / literal runs and passes the code runs
 // through `on_code`; comments are kept (or blanked), literals kept.
@@ -230,6 +237,85 @@ std::string compile_options_key(const std::vector<std::string> &opts)
 std::mutex g_cache_mutex;
 std::unordered_map<std::string, std::shared_ptr<const Program>> g_cache;
 
+// ---- on-disk cubin cache --------------------------------------------------
+// Directory: $SODECL_B200_CACHE_DIR, else `_cache` next to this library
+// (so programs built once travel with the package); disabled when the
+// variable is set to an empty string or the directory cannot be made.
+// Entry name = two 64-bit FNV-1a hashes of the full key (options + source);
+// each entry stores the key and is used only when it matches byte for byte.
+
+std::string cache_dir()
+{
+    const char *env = std::getenv("SODECL_B200_CACHE_DIR");
+    if (env) return env;
+    Dl_info info{};
+    if (dladdr(reinterpret_cast<void *>(&cache_dir), &info) && info.dli_fname) {
+        std::string path(info.dli_fname);
+        const size_t slash = path.rfind('/');
+        return (slash == std::string::npos ? std::string(".") : path.substr(0, slash)) + "/_cache";
+    }
+    return std::string();
+}
+
+uint64_t fnv1a(const std::string &s, uint64_t h)
+{
+    for (unsigned char c : s) {
+        h ^= c;
+        h *= 1099511628211ULL;
+    }
+    return h;
+}
+
+std::string cache_path(const std::string &key)
+{
+    const std::string dir = cache_dir();
+    if (dir.empty()) return std::string();
+    mkdir(dir.c_str(), 0755);
+    char name[64];
+    std::snprintf(name, sizeof(name), "/%016llx%016llx.cubin", (unsigned long long)fnv1a(key, 1469598103934665603ULL),
+                  (unsigned long long)fnv1a(key, 0x9E3779B97F4A7C15ULL));
+    return dir + name;
+}
+
+bool cache_load(const std::string &key, Program &prog)
+{
+    const std::string path = cache_path(key);
+    if (path.empty()) return false;
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return false;
+    uint64_t sizes[3];
+    if (!f.read(reinterpret_cast<char *>(sizes), sizeof(sizes))) return false;
+    if (sizes[0] != key.size() || sizes[1] > (1ull << 30) || sizes[2] > (1ull << 26)) return false;
+    std::string stored(sizes[0], '\0');
+    if (!f.read(&stored[0], sizes[0]) || stored != key) return false;
+    prog.cubin.resize(sizes[1]);
+    prog.log.resize(sizes[2]);
+    if (!f.read(prog.cubin.data(), sizes[1])) return false;
+    if (sizes[2] && !f.read(&prog.log[0], sizes[2])) return false;
+    return true;
+}
+
+void cache_store(const std::string &key, const Program &prog)
+{
+    const std::string path = cache_path(key);
+    if (path.empty()) return;
+    const std::string tmp = path + ".tmp" + std::to_string(getpid());
+    {
+        std::ofstream f(tmp, std::ios::binary);
+        if (!f) return;
+        const uint64_t sizes[3] = {key.size(), prog.cubin.size(), prog.log.size()};
+        f.write(reinterpret_cast<const char *>(sizes), sizeof(sizes));
+        f.write(key.data(), key.size());
+        f.write(prog.cubin.data(), prog.cubin.size());
+        f.write(prog.log.data(), prog.log.size());
+        if (!f) {
+            std::remove(tmp.c_str());
+            return;
+        }
+    }
+    std::rename(tmp.c_str(), path.c_str());
+}
+
 }  // namespace
 
 std::string print_like_reference(double x)
@@ -262,12 +348,13 @@ std::string assemble(const ProgramSpec &spec, const std::string &system_src, con
     s << "#define SODECL_SOLVER " << spec.solver << "\n";
     s << "#define SODECL_FP32 " << (spec.fp32 ? 1 : 0) << "\n";
     s << "#define SODECL_RECORD_F32 " << (spec.record_f32 ? 1 : 0) << "\n";
+    s << "#define SODECL_FAST_DIV " << (spec.fast_div ? 1 : 0) << "\n";
     s << "#define SODECL_HAS_JACOBIAN " << (traits.has_jacobian ? 1 : 0) << "\n";
     s << "#define SODECL_HAS_STOCH " << (traits.has_stoch ? 1 : 0) << "\n";
     s << "#define SODECL_NEWTON_MAX " << spec.newton_max_iter << "\n";
     s << "#define SODECL_BLOCK_MAX " << spec.block_max << "\n";
     if (spec.min_blocks > 0) s << "#define SODECL_MIN_BLOCKS " << spec.min_blocks << "\n";
-    s << kPreludeSrc << "\n" << kThreefrySrc << "\n";
+    s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n";
     // the reference's program defines (src/sodeclmgr.cpp:379-430); _listsize_
     // only when the system file names it, so one program serves every size
     s << "#define _numnoi_ " << spec.num_noi << "\n";
@@ -283,25 +370,29 @@ std::string assemble(const ProgramSpec &spec, const std::string &system_src, con
     if (spec.fp32) eps = suffix_in_code(eps);
     s << "#define _epsilon1_ " << eps << "\n";
     if (spec.fp32) s << "#define double float\n";
+    else if (spec.fast_div) s << "#define double sodecl_f64\n";
     s << "#line 1 \"system.cl\"\n";
     const std::string user = relax_parameter_bounds(system_src);
     s << (spec.fp32 ? suffix_float_literals(user) : user) << "\n";
-    if (spec.fp32) s << "#undef double\n";
+    if (spec.fp32 || spec.fast_div) s << "#undef double\n";
     s << "#line 1 \"solvers.cuh\"\n" << kSolversSrc << "\n";
     return s.str();
 }
 
-std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string &system_src)
+namespace {
+
+std::shared_ptr<const Program> compile_text(std::string source, bool fmad, bool fast_div, const char *kernel)
 {
-    const SystemTraits traits = inspect_system(system_src);
     auto prog = std::make_shared<Program>();
-    prog->source = assemble(spec, system_src, traits);
+    prog->source = std::move(source);
+    prog->fast_div = fast_div;
+    prog->kernel_name = kernel;
 
     std::vector<std::string> opts = {
         "--gpu-architecture=sm_100a",
         "--device-as-default-execution-space",
         "--std=c++17",
-        spec.fmad ? "--fmad=true" : "--fmad=false",
+        fmad ? "--fmad=true" : "--fmad=false",
         "--generate-line-info",
         "--ptxas-options=-v",
     };
@@ -310,6 +401,13 @@ std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string 
         std::lock_guard<std::mutex> lock(g_cache_mutex);
         auto it = g_cache.find(key);
         if (it != g_cache.end()) return it->second;
+    }
+
+    if (cache_load(key, *prog)) {
+        std::shared_ptr<const Program> done = prog;
+        std::lock_guard<std::mutex> lock(g_cache_mutex);
+        g_cache.emplace(key, done);
+        return done;
     }
 
     nvrtcProgram p = nullptr;
@@ -335,11 +433,148 @@ std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string 
     prog->cubin.resize(cubin_size);
     nvrtcGetCUBIN(p, prog->cubin.data());
     nvrtcDestroyProgram(&p);
+    cache_store(key, *prog);
 
     std::shared_ptr<const Program> done = prog;
     std::lock_guard<std::mutex> lock(g_cache_mutex);
     g_cache.emplace(key, done);
     return done;
+}
+
+std::shared_ptr<const Program> compile_one(const ProgramSpec &spec, const std::string &system_src,
+                                           const SystemTraits &traits)
+{
+    return compile_text(assemble(spec, system_src, traits), spec.fmad, spec.fast_div, "sodecl_orbits");
+}
+
+// Names of the object-like and function-like macros a source #defines, so a
+// batch program can #undef them after each class.
+std::vector<std::string> defined_macros(const std::string &src)
+{
+    std::vector<std::string> names;
+    const std::regex def("^[ \\t]*#[ \\t]*define[ \\t]+([A-Za-z_][A-Za-z0-9_]*)");
+    const std::string stripped = scan_code(src, [](const std::string &x) { return x; }, false);
+    for (std::sregex_iterator it(stripped.begin(), stripped.end(), def), end; it != end; ++it)
+        names.push_back((*it)[1].str());
+    return names;
+}
+
+std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div, int block_max)
+{
+    std::ostringstream s;
+    s << "// SODECL batch program generated by libsodecl_cuda (sm_100a)\n";
+    s << "#define SODECL_STEPS_ONLY 1\n#define SODECL_FP32 0\n#define SODECL_RECORD_F32 0\n";
+    s << "#define SODECL_FAST_DIV " << (fast_div ? 1 : 0) << "\n";
+    s << "#define SODECL_BLOCK_MAX " << block_max << "\n";
+    s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n" << kBatchSrc << "\n";
+    static const char *per_class[] = {"SODECL_SOLVER", "SODECL_HAS_JACOBIAN", "SODECL_HAS_STOCH", "SODECL_NEWTON_MAX",
+                                      "_numnoi_", "_numsteps_", "_m_dt_", "_numeq_", "_numpar_", "_epsilon1_",
+                                      "_listsize_", "SODECL_BATCH_CLASS_BODY"};
+    for (size_t k = 0; k < classes.size(); ++k) {
+        const ProgramSpec &sp = classes[k].spec;
+        const std::string &src = classes[k].system_src;
+        const SystemTraits tr = inspect_system(src);
+        s << "\n// ---- class " << k << "\n";
+        for (const char *m : per_class) s << "#undef " << m << "\n";
+        s << "#define SODECL_SOLVER " << sp.solver << "\n";
+        s << "#define SODECL_HAS_JACOBIAN " << (tr.has_jacobian ? 1 : 0) << "\n";
+        s << "#define SODECL_HAS_STOCH " << (tr.has_stoch ? 1 : 0) << "\n";
+        s << "#define SODECL_NEWTON_MAX " << sp.newton_max_iter << "\n";
+        s << "#define _numnoi_ " << sp.num_noi << "\n";
+        s << "#define _listsize_ " << sp.list_size << "\n";
+        s << "#define _numsteps_ 1\n";
+        s << "#define _m_dt_ " << print_like_reference(sp.dt) << "\n";
+        s << "#define _numeq_ " << sp.num_equat << "\n";
+        s << "#define _numpar_ " << sp.num_params << "\n";
+        s << "#define _epsilon1_ " << print_like_reference(sp.newton_tol) << "\n";
+        s << "namespace sodecl_cls_" << k << " {\n";
+        if (fast_div) s << "#define double sodecl_f64\n";
+        s << "#line 1 \"class" << k << ".cl\"\n" << relax_parameter_bounds(src) << "\n";
+        if (fast_div) s << "#undef double\n";
+        for (const auto &m : defined_macros(src)) s << "#undef " << m << "\n";
+        s << "#line 1 \"solvers.cuh\"\n" << kSolversSrc << "\n";
+        s << "#define SODECL_BATCH_CLASS_BODY 1\n#line 1 \"batch.cuh\"\n" << kBatchSrc << "\n";
+        s << "}  // namespace sodecl_cls_" << k << "\n";
+    }
+    s << "\nextern \"C\" __global__ void __launch_bounds__(SODECL_BLOCK_MAX) sodecl_batch(const sodecl_batch_args a)\n{\n";
+    s << "    for (int k = 0; k < a.nclasses; ++k) {\n        switch (a.order[k]) {\n";
+    for (size_t k = 0; k < classes.size(); ++k)
+        s << "        case " << k << ": sodecl_cls_" << k << "::sodecl_class_run(a, " << k << "); break;\n";
+    s << "        default: break;\n        }\n    }\n}\n";
+    return s.str();
+}
+
+std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, int tape_cap)
+{
+    const SystemTraits tr = inspect_system(src);
+    std::ostringstream s;
+    s << "// SODECL adjoint program generated by libsodecl_cuda (sm_100a)\n";
+    s << "#define SODECL_STEPS_ONLY 1\n#define SODECL_FP32 0\n#define SODECL_RECORD_F32 0\n#define SODECL_FAST_DIV 0\n";
+    s << "#define SODECL_SOLVER " << spec.solver << "\n";
+    s << "#define SODECL_HAS_JACOBIAN " << (tr.has_jacobian ? 1 : 0) << "\n";
+    s << "#define SODECL_HAS_STOCH " << (tr.has_stoch ? 1 : 0) << "\n";
+    s << "#define SODECL_NEWTON_MAX " << spec.newton_max_iter << "\n";
+    s << "#define SODECL_BLOCK_MAX " << spec.block_max << "\n";
+    s << "#define SODECL_TAPE_CAP " << tape_cap << "\n";
+    s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n" << kAdjointSrc << "\n";
+    s << "#define _numnoi_ " << spec.num_noi << "\n";
+    s << "#define _listsize_ " << spec.list_size << "\n";
+    s << "#define _numsteps_ " << spec.kernel_steps << "\n";
+    s << "#define _m_dt_ " << print_like_reference(spec.dt) << "\n";
+    s << "#define _numeq_ " << spec.num_equat << "\n";
+    s << "#define _numpar_ " << spec.num_params << "\n";
+    s << "#define _epsilon1_ " << print_like_reference(spec.newton_tol) << "\n";
+    const std::string user = relax_parameter_bounds(src);
+    const std::vector<std::string> macros = defined_macros(src);
+    s << "#line 1 \"system.cl\"\n" << user << "\n";
+    for (const auto &m : macros) s << "#undef " << m << "\n";
+    // the recording copy: every double of the system file is a sodecl_ad
+    s << "namespace sodecl_adsys {\n#define double sodecl_ad\n#line 1 \"system.cl\"\n" << user
+      << "\n#undef double\n}  // namespace sodecl_adsys\n";
+    for (const auto &m : macros) s << "#undef " << m << "\n";
+    s << "#line 1 \"solvers.cuh\"\n" << kSolversSrc << "\n";
+    s << "#define SODECL_ADJOINT_KERNEL 1\n#line 1 \"adjoint.cuh\"\n" << kAdjointSrc << "\n";
+    return s.str();
+}
+
+}  // namespace
+
+std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std::string &system_src, int tape_cap)
+{
+    return compile_text(assemble_adjoint(spec, system_src, tape_cap), spec.fmad, false, "sodecl_adjoint");
+}
+
+std::shared_ptr<const Program> build_batch(const std::vector<BatchClass> &classes, bool fmad, bool fast_div,
+                                           int block_max)
+{
+    if (classes.empty()) throw std::runtime_error("a batch needs at least one class");
+    bool fd = fast_div;
+    for (const auto &c : classes)
+        if (c.system_src.find("printf") != std::string::npos) fd = false;
+    if (fd) {
+        try {
+            return compile_text(assemble_batch(classes, true, block_max), fmad, true, "sodecl_batch");
+        } catch (const std::exception &) {
+        }
+    }
+    return compile_text(assemble_batch(classes, false, block_max), fmad, false, "sodecl_batch");
+}
+
+std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string &system_src)
+{
+    const SystemTraits traits = inspect_system(system_src);
+    ProgramSpec s = spec;
+    if (s.fp32) s.fast_div = false;
+    // the wrapper type would hand a struct to printf's varargs
+    if (s.fast_div && system_src.find("printf") != std::string::npos) s.fast_div = false;
+    if (!s.fast_div) return compile_one(s, system_src, traits);
+    try {
+        return compile_one(s, system_src, traits);
+    } catch (const std::exception &) {
+        // the system file needs plain `double` (an implicit conversion, say)
+        s.fast_div = false;
+        return compile_one(s, system_src, traits);
+    }
 }
 
 }  // namespace sodecl_b200

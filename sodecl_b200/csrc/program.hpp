@@ -19,6 +19,7 @@ struct ProgramSpec {
     bool fp32 = false;
     bool fmad = true;
     bool record_f32 = false;
+    bool fast_div = false;   // FP64 through sodecl_f64 (exact reciprocal quotients)
     double newton_tol = 1e-7;
     int newton_max_iter = 1000;
     int block_max = 256;
@@ -30,6 +31,7 @@ struct Program {
     std::string log;         // NVRTC log (with ptxas resource usage)
     std::vector<char> cubin;
     std::string kernel_name = "sodecl_orbits";
+    bool fast_div = false;   // built with the reciprocal-division wrapper
 };
 
 // What the system file provides.
@@ -56,5 +58,21 @@ std::string assemble(const ProgramSpec &spec, const std::string &system_src, con
 // Compiles (or returns from the process-wide cache) the program.  Throws
 // std::runtime_error with the NVRTC log on failure.
 std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string &system_src);
+
+// The discrete-adjoint program (kernel `sodecl_adjoint`) for the Euler or RK4
+// solver: the system file twice, plain and with `double` recording on a tape
+// of `tape_cap` entries per right-hand-side evaluation.
+std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std::string &system_src, int tape_cap);
+
+// One class of a heterogeneous batch: a system file with a solver, sizes,
+// step and Newton settings (kernel_steps/list_size unused).
+struct BatchClass {
+    ProgramSpec spec;
+    std::string system_src;
+};
+
+// All classes in one program with the persistent kernel `sodecl_batch`.
+std::shared_ptr<const Program> build_batch(const std::vector<BatchClass> &classes, bool fmad, bool fast_div,
+                                           int block_max);
 
 }  // namespace sodecl_b200

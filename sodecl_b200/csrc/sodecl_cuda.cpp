@@ -48,6 +48,25 @@ struct DeviceArgs {
     int *flags;
 };
 
+// Must match struct sodecl_adjoint_args in device/adjoint.cuh field for field.
+struct AdjointArgs {
+    const double *t0;
+    const double *y0;
+    const double *p;
+    const double *targets;
+    double *loss;
+    double *grad_p;
+    double *grad_y0;
+    double *ckpt;
+    double *ckpt_t;
+    double *seg;
+    double *seg_t;
+    int *flags;
+    long long n;
+    int nchunks;
+    int ckpt_every;
+};
+
 constexpr int kDefaultBlock = 128;
 constexpr int kMaxCopyGroups = 8;
 
@@ -76,6 +95,14 @@ struct sodecl_ctx {
 
     double last_kernel_ms = 0.0;
     double last_total_ms = 0.0;
+
+    // discrete adjoint: its own program and scratch (checkpoints, segments)
+    std::shared_ptr<const Program> adj_prog;
+    cudaLibrary_t adj_lib = nullptr;
+    cudaKernel_t adj_kernel = nullptr;
+    int adj_tape = 0;
+    void *adj_scratch = nullptr;
+    size_t adj_scratch_bytes = 0;
 
     int fail(int code, const std::string &msg)
     {
@@ -196,6 +223,27 @@ int launch(sodecl_ctx *ctx, const DeviceArgs &a, cudaStream_t stream)
     return SODECL_OK;
 }
 
+ProgramSpec make_spec(const sodecl_cfg &c)
+{
+    ProgramSpec spec;
+    spec.solver = c.solver;
+    spec.num_equat = c.num_equat;
+    spec.num_params = c.num_params;
+    spec.num_noi = c.num_noi;
+    spec.list_size = c.list_size;
+    spec.kernel_steps = c.kernel_steps;
+    spec.dt = c.dt;
+    spec.fp32 = c.precision == SODECL_FP32;
+    spec.fmad = c.fmad != 0;
+    spec.record_f32 = c.record_f32 != 0;
+    spec.newton_tol = c.newton_tol;
+    spec.newton_max_iter = c.newton_max_iter;
+    spec.block_max = std::max(256, c.local_group_size > 0 ? c.local_group_size : kDefaultBlock);
+    spec.min_blocks = c.min_blocks_per_sm;
+    spec.fast_div = c.division == SODECL_DIV_RECIPROCAL;
+    return spec;
+}
+
 }  // namespace
 
 extern "C" {
@@ -210,6 +258,7 @@ void sodecl_cfg_init(sodecl_cfg *cfg)
     cfg->fmad = 1;
     cfg->newton_tol = 1e-7;
     cfg->newton_max_iter = 1000;
+    cfg->division = SODECL_DIV_IEEE;
 }
 
 int sodecl_cuda_abi_version(void) { return SODECL_CUDA_ABI_VERSION; }
@@ -259,6 +308,7 @@ int sodecl_cuda_create(const sodecl_cfg *cfg, sodecl_ctx **out)
     if (c.local_group_size < 0 || c.local_group_size > 1024) return SODECL_ERR_INVALID_ARG;
     if (c.newton_tol < 0 || !std::isfinite(c.newton_tol) || c.newton_max_iter < 0) return SODECL_ERR_INVALID_ARG;
     if (c.min_blocks_per_sm < 0 || c.min_blocks_per_sm > 32) return SODECL_ERR_INVALID_ARG;
+    if (c.division != SODECL_DIV_RECIPROCAL && c.division != SODECL_DIV_IEEE) return SODECL_ERR_INVALID_ARG;
     const int64_t nchunks = count_chunks(c);
     if (nchunks > 0x7ffffffeLL) return SODECL_ERR_INVALID_ARG;
     auto *ctx = new (std::nothrow) sodecl_ctx();
@@ -283,21 +333,7 @@ int sodecl_cuda_compile(sodecl_ctx *ctx, const char *system_src, size_t len)
         return ctx->fail(SODECL_ERR_NO_JACOBIAN, "implicit solvers need calc_jacobian(...) in the system file");
     if (solver == SODECL_STOCHASTIC_EULER && !traits.has_stoch)
         return ctx->fail(SODECL_ERR_NO_STOCH, "the stochastic solver needs sode_system_stoch(...) in the system file");
-    ProgramSpec spec;
-    spec.solver = solver;
-    spec.num_equat = ctx->cfg.num_equat;
-    spec.num_params = ctx->cfg.num_params;
-    spec.num_noi = ctx->cfg.num_noi;
-    spec.list_size = ctx->cfg.list_size;
-    spec.kernel_steps = ctx->cfg.kernel_steps;
-    spec.dt = ctx->cfg.dt;
-    spec.fp32 = ctx->cfg.precision == SODECL_FP32;
-    spec.fmad = ctx->cfg.fmad != 0;
-    spec.record_f32 = ctx->cfg.record_f32 != 0;
-    spec.newton_tol = ctx->cfg.newton_tol;
-    spec.newton_max_iter = ctx->cfg.newton_max_iter;
-    spec.block_max = std::max(256, block_size(ctx));
-    spec.min_blocks = ctx->cfg.min_blocks_per_sm;
+    ProgramSpec spec = make_spec(ctx->cfg);
     try {
         auto prog = sodecl_b200::build(spec, src);
         if (ctx->gpu_ready && prog != ctx->prog) {
@@ -554,6 +590,218 @@ int sodecl_cuda_kernel_info(sodecl_ctx *ctx, int *regs, int *local_bytes, int *m
     return SODECL_OK;
 }
 
+int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_steps, int32_t *block,
+                         int32_t *min_blocks, int32_t *division, double *best_ms)
+{
+    if (!ctx) return SODECL_ERR_INVALID_ARG;
+    if (!ctx->uploaded) return ctx->fail(SODECL_ERR_STATE, "upload the orbits first: the tuner samples them");
+    if (sample_orbits < 1 || sample_steps < 1) return ctx->fail(SODECL_ERR_INVALID_ARG, "empty sample");
+    DeviceScope dev(ctx->cfg.device);
+    const int64_t n = std::min<int64_t>(sample_orbits, ctx->cfg.list_size);
+    const size_t neq = ctx->cfg.num_equat, npar = std::max(1, ctx->cfg.num_params);
+    const int chunks = std::max<int>(1, (sample_steps + ctx->cfg.kernel_steps - 1) / ctx->cfg.kernel_steps);
+    // scratch copies of the sample, so the real state does not advance
+    double *t = nullptr, *y = nullptr, *cnt = nullptr;
+    SODECL_CUDA_TRY(ctx, cudaMalloc(&t, n * sizeof(double)));
+    struct Free {
+        void *p[3];
+        ~Free() { for (void *q : p) cudaFree(q); }
+    } guard{{t, nullptr, nullptr}};
+    SODECL_CUDA_TRY(ctx, cudaMalloc(&y, n * neq * sizeof(double)));
+    guard.p[1] = y;
+    SODECL_CUDA_TRY(ctx, cudaMalloc(&cnt, n * sizeof(double)));
+    guard.p[2] = cnt;
+    (void)npar;
+
+    struct Cand {
+        int block, min_blocks, division;
+    };
+    std::vector<Cand> cands = {{128, 0, SODECL_DIV_IEEE}, {128, 4, SODECL_DIV_IEEE}, {256, 3, SODECL_DIV_IEEE},
+                               {64, 0, SODECL_DIV_IEEE}};
+    if (ctx->cfg.precision == SODECL_FP64) {
+        cands.push_back({128, 0, SODECL_DIV_RECIPROCAL});
+        cands.push_back({128, 4, SODECL_DIV_RECIPROCAL});
+    }
+    const sodecl_cfg saved = ctx->cfg;
+    auto saved_prog = ctx->prog;
+    double best = 1e300;
+    Cand pick = {saved.local_group_size > 0 ? saved.local_group_size : kDefaultBlock, saved.min_blocks_per_sm,
+                 saved.division};
+    cudaEvent_t e0, e1;
+    SODECL_CUDA_TRY(ctx, cudaEventCreate(&e0));
+    SODECL_CUDA_TRY(ctx, cudaEventCreate(&e1));
+    int rc = SODECL_OK;
+    for (const Cand &c : cands) {
+        sodecl_cfg cfg = saved;
+        cfg.local_group_size = c.block;
+        cfg.min_blocks_per_sm = c.min_blocks;
+        cfg.division = c.division;
+        std::shared_ptr<const Program> prog;
+        try {
+            prog = sodecl_b200::build(make_spec(cfg), ctx->system_src);
+        } catch (const std::exception &ex) {
+            continue;
+        }
+        if (c.division == SODECL_DIV_RECIPROCAL && !prog->fast_div) continue;  // fell back to IEEE
+        cudaLibrary_t lib = nullptr;
+        cudaKernel_t kern = nullptr;
+        if (cudaLibraryLoadData(&lib, prog->cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0) != cudaSuccess ||
+            cudaLibraryGetKernel(&kern, lib, prog->kernel_name.c_str()) != cudaSuccess) {
+            cudaGetLastError();
+            if (lib) cudaLibraryUnload(lib);
+            continue;
+        }
+        float ms = 0.f;
+        for (int rep = 0; rep < 2 && rc == SODECL_OK; ++rep) {
+            cudaMemcpyAsync(t, ctx->d_t, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+            cudaMemcpyAsync(y, ctx->d_y, n * neq * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+            cudaMemcpyAsync(cnt, ctx->d_cnt, n * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream);
+            DeviceArgs a{};
+            a.t = t;
+            a.y = y;
+            a.p = ctx->d_p;
+            a.counters = cnt;
+            a.n = n;
+            a.rec_stride = n;
+            a.chunk_begin = 0;
+            a.chunk_end = chunks;
+            void *args[] = {&a};
+            cudaEventRecord(e0, ctx->stream);
+            cudaError_t le = cudaLaunchKernel(reinterpret_cast<const void *>(kern),
+                                              dim3(static_cast<unsigned>((n + c.block - 1) / c.block)), dim3(c.block),
+                                              args, 0, ctx->stream);
+            cudaEventRecord(e1, ctx->stream);
+            if (le != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+                rc = cuda_fail(ctx, le != cudaSuccess ? le : cudaErrorUnknown, "autotune launch");
+                break;
+            }
+            cudaEventElapsedTime(&ms, e0, e1);
+        }
+        cudaLibraryUnload(lib);
+        if (rc != SODECL_OK) break;
+        if (ms < best) {
+            best = ms;
+            pick = c;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != SODECL_OK) return rc;
+    // rebuild the context's program with the winner
+    ctx->cfg.local_group_size = pick.block;
+    ctx->cfg.min_blocks_per_sm = pick.min_blocks;
+    ctx->cfg.division = pick.division;
+    try {
+        auto prog = sodecl_b200::build(make_spec(ctx->cfg), ctx->system_src);
+        if (prog != ctx->prog) {
+            if (ctx->lib) cudaLibraryUnload(ctx->lib);
+            ctx->lib = nullptr;
+            ctx->kernel = nullptr;
+            ctx->gpu_ready = false;
+            ctx->prog = prog;
+        }
+    } catch (const std::exception &ex) {
+        ctx->cfg = saved;
+        ctx->prog = saved_prog;
+        return ctx->fail(SODECL_ERR_COMPILE, ex.what());
+    }
+    if ((rc = ensure_gpu(ctx)) != SODECL_OK) return rc;
+    if (block) *block = pick.block;
+    if (min_blocks) *min_blocks = pick.min_blocks;
+    if (division) *division = pick.division;
+    if (best_ms) *best_ms = best;
+    return SODECL_OK;
+}
+
+int sodecl_cuda_program_division(const sodecl_ctx *ctx)
+{
+    if (!ctx || !ctx->prog) return SODECL_ERR_STATE;
+    return ctx->prog->fast_div ? SODECL_DIV_RECIPROCAL : SODECL_DIV_IEEE;
+}
+
+int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stream)
+{
+    if (!ctx) return SODECL_ERR_INVALID_ARG;
+    if (!io || !io->t0 || !io->y0 || (!io->params && ctx->cfg.num_params > 0) || !io->targets || !io->loss)
+        return ctx->fail(SODECL_ERR_INVALID_ARG, "adjoint: t0, y0, params, targets and loss are required");
+    if (ctx->cfg.solver != SODECL_EULER && ctx->cfg.solver != SODECL_RUNGE_KUTTA)
+        return ctx->fail(SODECL_ERR_UNSUPPORTED, "the adjoint covers the Euler and RK4 solvers");
+    if (ctx->cfg.precision != SODECL_FP64) return ctx->fail(SODECL_ERR_UNSUPPORTED, "the adjoint is FP64");
+    if (io->n < 1 || io->n > ctx->cfg.list_size) return ctx->fail(SODECL_ERR_INVALID_ARG, "adjoint: orbit count");
+    if (io->tape_entries < 0 || io->tape_entries > 30000)
+        return ctx->fail(SODECL_ERR_INVALID_ARG, "adjoint: tape size out of range");
+    if (ctx->system_src.empty()) return ctx->fail(SODECL_ERR_STATE, "compile the system first");
+    DeviceScope dev(ctx->cfg.device);
+    const int tape = io->tape_entries > 0 ? io->tape_entries : 256;
+    if (!ctx->adj_prog || ctx->adj_tape != tape) {
+        try {
+            ProgramSpec spec = make_spec(ctx->cfg);
+            auto prog = sodecl_b200::build_adjoint(spec, ctx->system_src, tape);
+            if (ctx->adj_lib) cudaLibraryUnload(ctx->adj_lib);
+            ctx->adj_lib = nullptr;
+            ctx->adj_kernel = nullptr;
+            ctx->adj_prog = prog;
+            ctx->adj_tape = tape;
+        } catch (const std::exception &ex) {
+            return ctx->fail(SODECL_ERR_COMPILE, ex.what());
+        }
+    }
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || ctx->cfg.device >= count) {
+        cudaGetLastError();
+        return ctx->fail(SODECL_ERR_NO_DEVICE, "no CUDA device");
+    }
+    if (!ctx->adj_lib) {
+        SODECL_CUDA_TRY(ctx, cudaLibraryLoadData(&ctx->adj_lib, ctx->adj_prog->cubin.data(), nullptr, nullptr, 0,
+                                                 nullptr, nullptr, 0));
+        SODECL_CUDA_TRY(ctx, cudaLibraryGetKernel(&ctx->adj_kernel, ctx->adj_lib, "sodecl_adjoint"));
+    }
+    const long long n = io->n;
+    const int64_t steps = ctx->nchunks * static_cast<int64_t>(ctx->cfg.kernel_steps);
+    int C = io->ckpt_every > 0 ? io->ckpt_every
+                               : std::max<int>(1, static_cast<int>(std::ceil(std::sqrt(static_cast<double>(steps)))));
+    if (steps > 0 && C > steps) C = static_cast<int>(steps);
+    const int64_t nckpt = steps > 0 ? (steps + C - 1) / C : 1;
+    const size_t neq = ctx->cfg.num_equat;
+    const size_t need = io->grad_params || io->grad_y0
+                            ? sizeof(double) * n * (nckpt * (neq + 1) + static_cast<int64_t>(C) * (neq + 1))
+                            : 0;
+    if (need > ctx->adj_scratch_bytes) {
+        cudaFree(ctx->adj_scratch);
+        ctx->adj_scratch = nullptr;
+        ctx->adj_scratch_bytes = 0;
+        SODECL_CUDA_TRY(ctx, cudaMalloc(&ctx->adj_scratch, need));
+        ctx->adj_scratch_bytes = need;
+    }
+    AdjointArgs a{};
+    a.t0 = io->t0;
+    a.y0 = io->y0;
+    a.p = io->params;
+    a.targets = io->targets;
+    a.loss = io->loss;
+    a.grad_p = io->grad_params;
+    a.grad_y0 = io->grad_y0;
+    if (need) {
+        double *base = static_cast<double *>(ctx->adj_scratch);
+        a.ckpt = base;
+        a.ckpt_t = a.ckpt + nckpt * neq * n;
+        a.seg = a.ckpt_t + nckpt * n;
+        a.seg_t = a.seg + static_cast<int64_t>(C) * neq * n;
+        // the kernel writes gradients only when grad_p is set; give it a sink
+        if (!a.grad_p) return ctx->fail(SODECL_ERR_INVALID_ARG, "adjoint: grad_params is required with grad_y0");
+    }
+    a.flags = io->flags;
+    a.n = n;
+    a.nchunks = static_cast<int>(ctx->nchunks);
+    a.ckpt_every = C;
+    const int block = 128;
+    void *args[] = {&a};
+    SODECL_CUDA_TRY(ctx, cudaLaunchKernel(reinterpret_cast<const void *>(ctx->adj_kernel),
+                                          dim3(static_cast<unsigned>((n + block - 1) / block)), dim3(block), args, 0,
+                                          static_cast<cudaStream_t>(stream)));
+    return SODECL_OK;
+}
+
 size_t sodecl_cuda_last_error(const sodecl_ctx *ctx, char *buf, size_t n)
 {
     return copy_string(ctx ? ctx->error : std::string("null context"), buf, n);
@@ -572,11 +820,13 @@ size_t sodecl_cuda_program_source(const sodecl_ctx *ctx, char *buf, size_t n)
 void sodecl_cuda_destroy(sodecl_ctx *ctx)
 {
     if (!ctx) return;
-    if (ctx->gpu_ready || ctx->uploaded) {
+    if (ctx->gpu_ready || ctx->uploaded || ctx->adj_lib) {
         DeviceScope dev(ctx->cfg.device);
         if (ctx->stream) cudaStreamSynchronize(ctx->stream);
         if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
         free_buffers(ctx);
+        cudaFree(ctx->adj_scratch);
+        if (ctx->adj_lib) cudaLibraryUnload(ctx->adj_lib);
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
         if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
         if (ctx->lib) cudaLibraryUnload(ctx->lib);

@@ -196,3 +196,18 @@ def test_python_module_fails_cleanly_without_device():
     out = sodecl_interface.sodeclcall([0.0], [0.0] * 6, [1.0] * 6, 0, 0, system_path("oculomotor"), 9, 1, 6, 6, 0,
                                       1e-3, 0.01, 10, 0)
     assert out == []
+
+
+def test_division_modes_and_fallback():
+    """FP64 programs build with the reciprocal quotient; a system file that
+    needs plain double (an implicit conversion) falls back to IEEE division."""
+    kw = dict(dt=1e-3, tspan=0.1, ksteps=10, neq=6, npar=6, orbits=4)
+    assert Integrator(system_path("oculomotor"), "rk4", division="reciprocal", **kw).division == "reciprocal"
+    assert Integrator(system_path("oculomotor"), "rk4", **kw).division == "ieee"
+    assert Integrator(system_path("oculomotor"), "rk4", division="reciprocal", precision="fp32", **kw).division == "ieee"
+    src = open(system_path("oculomotor")).read().replace("double drive = y[3] - y[4];", "float drive = y[3] - y[4];")
+    sim = Integrator(None, "rk4", system_src=src, division="reciprocal", **kw)
+    assert sim.division == "ieee"
+    assert "#define SODECL_FAST_DIV 0" in sim.program_source
+    text = Integrator(system_path("oculomotor"), "rk4", division="reciprocal", **kw).program_source
+    assert "#define SODECL_FAST_DIV 1" in text and "#define double sodecl_f64" in text

@@ -1,0 +1,131 @@
+"""Discrete adjoint (model fitting): loss and d(loss)/d(params, y0) per orbit.
+
+The GPU adjoint (sodecl_cuda_adjoint) is checked against
+  * an FP64 reference gradient: forward-mode dual numbers through the same
+    system file and a restatement of the steps (oracle/gradient.cpp), which is
+    exact to rounding -- agreement to 1e-9 of the gradient's scale;
+  * central finite differences of the GPU loss (relative step 1e-6), the
+    baseline the adjoint is meant to replace -- agreement to 1e-6.
+The per-orbit loss is checked against the CPU oracle's records."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, reference_gradient
+
+NOMINAL = np.array([120.0, 1.5, 0.0045, 0.05, 600.0, 9.0])
+Y0 = np.array([0.0, 0.0, 0.0, 0.0, 0.0, 2.0])
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SYSTEMS = os.path.join(REPO, "sodecl_b200", "systems")
+
+
+def fitting_problem(n, seed, dt=1e-5, nchunks=10, ksteps=50, noise=1e-2):
+    """Targets: trajectories of perturbed true parameters plus Gaussian noise."""
+    rng = np.random.default_rng(seed)
+    true_p = NOMINAL * rng.uniform(0.5, 1.5, (n, 6))
+    y0 = np.tile(Y0, (n, 1))
+    rec = Oracle("oculomotor").run(2, np.zeros(n), y0, true_p, neq=6, npar=6, dt=dt, ksteps=ksteps,
+                                   nchunks=nchunks).records
+    targets = rec + rng.normal(0, noise, rec.shape)
+    guess = true_p * rng.uniform(0.95, 1.05, (n, 6))
+    return np.zeros(n), y0, guess, targets
+
+
+def test_reference_gradient_matches_cpu_finite_differences():
+    t0, y0, p, tg = fitting_problem(2, 0, nchunks=4, ksteps=25)
+    kw = dict(neq=6, npar=6, dt=1e-5, ksteps=25, nchunks=4)
+    loss, gp, gy = reference_gradient(os.path.join(SYSTEMS, "oculomotor.cl"), 2, 6, 6, 1e-5, 25, 4, t0, y0, p, tg)
+    o = Oracle("oculomotor")
+
+    def cpu_loss(pp, yy):
+        rec = o.run(2, t0, yy, pp, **kw).records
+        return ((rec - tg) ** 2).sum(axis=(0, 1)) / (5 * 6)
+
+    assert np.allclose(cpu_loss(p, y0), loss, rtol=1e-13)
+    for j in range(6):
+        h = 1e-6 * abs(p[0, j])
+        pp, pm = p.copy(), p.copy()
+        pp[:, j] += h
+        pm[:, j] -= h
+        fd = (cpu_loss(pp, y0) - cpu_loss(pm, y0)) / (2 * h)
+        assert np.allclose(fd, gp[:, j], rtol=1e-5, atol=1e-9 * np.abs(gp).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("solver", ["rk4", "euler"])
+def test_adjoint_matches_reference_gradient(solver):
+    torch = pytest.importorskip("torch")
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.fit import Adjoint
+
+    n, nchunks, ksteps, dt = 64, 10, 50, 1e-5 if solver == "rk4" else 1e-6
+    t0, y0, p, tg = fitting_problem(n, 1, dt=dt, nchunks=nchunks, ksteps=ksteps)
+    sid = 2 if solver == "rk4" else 1
+    loss_r, gp_r, gy_r = reference_gradient(system_path("oculomotor"), sid, 6, 6, dt, ksteps, nchunks, t0[:8], y0[:8],
+                                            p[:8], tg[:, :, :8])
+    sim = Integrator(system_path("oculomotor"), solver, dt=dt, tspan=nchunks * ksteps * dt, ksteps=ksteps, neq=6,
+                     npar=6, orbits=n)
+    assert sim.num_chunks == nchunks
+    dev = torch.device("cuda")
+    T = lambda a: torch.tensor(a, device=dev)  # noqa: E731
+    loss, gp, gy, flags = Adjoint(sim)(T(t0), T(y0), T(p), T(tg))
+    loss, gp, gy = loss.cpu().numpy(), gp.cpu().numpy(), gy.cpu().numpy()
+    assert not flags.any()
+    np.testing.assert_allclose(loss[:8], loss_r, rtol=1e-11)
+    scale_p = np.abs(gp_r).max(axis=1, keepdims=True)
+    scale_y = np.abs(gy_r).max(axis=1, keepdims=True)
+    assert np.max(np.abs(gp[:8] - gp_r) / scale_p) < 1e-9
+    assert np.max(np.abs(gy[:8] - gy_r) / scale_y) < 1e-9
+
+
+@pytest.mark.gpu
+def test_adjoint_against_finite_differences_and_checkpoint_spacing():
+    torch = pytest.importorskip("torch")
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.fit import Adjoint, finite_difference_gradient
+
+    n, nchunks, ksteps, dt = 256, 20, 25, 1e-5
+    t0, y0, p, tg = fitting_problem(n, 2, dt=dt, nchunks=nchunks, ksteps=ksteps)
+    kw = dict(dt=dt, tspan=nchunks * ksteps * dt, ksteps=ksteps, neq=6, npar=6)
+    dev = torch.device("cuda")
+    T = lambda a: torch.tensor(a, device=dev)  # noqa: E731
+    sim = Integrator(system_path("oculomotor"), "rk4", orbits=n, **kw)
+    grads = [Adjoint(sim, ckpt_every=c)(T(t0), T(y0), T(p), T(tg)) for c in (0, 1, 7, 500)]
+    for g in grads[1:]:  # recomputation is exact: same gradients for any spacing
+        assert torch.equal(g[1], grads[0][1]) and torch.equal(g[2], grads[0][2])
+    wide = Integrator(system_path("oculomotor"), "rk4", orbits=n * 24, **kw)
+    fd_p, fd_y = finite_difference_gradient(T(t0), T(y0), T(p), T(tg), Adjoint(wide))
+    gp, gy = grads[0][1], grads[0][2]
+    err_p = ((gp - fd_p).abs().amax(dim=1) / gp.abs().amax(dim=1)).max().item()
+    err_y = ((gy - fd_y).abs().amax(dim=1) / gy.abs().amax(dim=1)).max().item()
+    print("adjoint vs central differences: params %.2e, y0 %.2e" % (err_p, err_y))
+    assert err_p < 1e-6 and err_y < 1e-6
+
+
+@pytest.mark.gpu
+def test_torch_autograd_function_and_tape_overflow():
+    torch = pytest.importorskip("torch")
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.fit import Adjoint, trajectory_mse
+
+    n, nchunks, ksteps, dt = 32, 5, 20, 1e-5
+    t0, y0, p, tg = fitting_problem(n, 3, dt=dt, nchunks=nchunks, ksteps=ksteps)
+    sim = Integrator(system_path("oculomotor"), "rk4", dt=dt, tspan=nchunks * ksteps * dt, ksteps=ksteps, neq=6,
+                     npar=6, orbits=n)
+    dev = torch.device("cuda")
+    params = torch.tensor(p, device=dev, requires_grad=True)
+    y0t = torch.tensor(y0, device=dev, requires_grad=True)
+    adj = Adjoint(sim)
+    loss = trajectory_mse(params, y0t, torch.tensor(t0, device=dev), torch.tensor(tg, device=dev), adj)
+    (2.0 * loss.sum()).backward()
+    _, gp, gy, _ = adj(torch.tensor(t0, device=dev), torch.tensor(y0, device=dev), torch.tensor(p, device=dev),
+                       torch.tensor(tg, device=dev))
+    assert torch.allclose(params.grad, 2.0 * gp) and torch.allclose(y0t.grad, 2.0 * gy)
+    # a tape too short for one right-hand side is reported, not silently wrong
+    _, _, _, flags = Adjoint(sim, tape_entries=16)(torch.tensor(t0, device=dev), torch.tensor(y0, device=dev),
+                                                    torch.tensor(p, device=dev), torch.tensor(tg, device=dev))
+    assert (flags.cpu().numpy() & 4).all()
+    with pytest.raises(RuntimeError):
+        trajectory_mse(params, y0t, torch.tensor(t0, device=dev), torch.tensor(tg, device=dev),
+                       Adjoint(sim, tape_entries=16))

@@ -1,0 +1,154 @@
+"""Heterogeneous batches: one persistent kernel over orbits of several system x
+solver classes with per-orbit step counts (sodecl_batch_* C ABI).
+
+Every orbit of a batch runs the same device code as the single-system kernel
+(sodecl_advance), so its final state must equal, bit for bit, what the
+single-system kernel gives for that orbit alone; that kernel is itself checked
+against the oracle in test_gpu_parity.py."""
+import re
+
+import numpy as np
+import pytest
+
+from sodecl_b200 import _native as N
+from sodecl_b200 import Integrator, system_path
+from sodecl_b200.batch import Batch
+
+NOMINAL = np.array([120.0, 1.5, 0.0045, 0.05, 600.0, 9.0])
+Y0 = np.array([0.0, 0.0, 0.0, 0.0, 0.0, 2.0])
+
+# (system, solver, neq, npar, nnoi, dt)
+CLASSES = [("kuramoto", "euler", 4, 5, 0, 0.01), ("kuramoto", "rk4", 16, 17, 0, 0.01),
+           ("kuramoto", "ie", 8, 9, 0, 0.01), ("oculomotor", "rk4", 6, 6, 0, 1e-5),
+           ("oculomotor", "ie", 6, 6, 0, 1e-3), ("kuramoto", "se", 5, 11, 5, 0.01)]
+
+
+def make_batch(fmad=True, classes=CLASSES):
+    b = Batch(fmad=fmad)
+    for system, solver, neq, npar, nnoi, dt in classes:
+        b.add_class(system_path(system), solver, neq=neq, npar=npar, nnoi=nnoi, dt=dt)
+    return b.compile()
+
+
+def make_items(n, seed, classes=CLASSES, steps=(0, 1, 7, 50, 123, 400)):
+    rng = np.random.default_rng(seed)
+    cls = rng.integers(0, len(classes), n).astype(np.int32)
+    nsteps = rng.choice(steps, n).astype(np.int64)
+    t0 = rng.uniform(0, 1, n)
+    y0, p = [], []
+    for c in cls:
+        system, solver, neq, npar, nnoi, dt = classes[c]
+        if system == "oculomotor":
+            y0.append(Y0.copy())
+            p.append(NOMINAL * rng.uniform(0.5, 1.5, 6))
+        else:
+            y0.append(rng.uniform(0, 2 * np.pi, neq))
+            q = np.concatenate([[rng.uniform(0, 5)], rng.normal(size=neq)])
+            if nnoi:
+                q = np.concatenate([q, rng.uniform(0, 0.5, nnoi)])
+            p.append(q)
+    counters = rng.integers(0, 2 ** 40, n).astype(float)
+    return cls, nsteps, t0, y0, p, counters
+
+
+def test_batch_program_builds_without_gpu():
+    b = make_batch()
+    text = b.program_source
+    assert len(re.findall(r"namespace sodecl_cls_\d+ \{", text)) == len(CLASSES)
+    assert "sodecl_batch(const sodecl_batch_args a)" in text
+    assert len(re.findall(r"case \d+: sodecl_cls_\d+::sodecl_class_run", text)) == len(CLASSES)
+
+
+def test_batch_validation():
+    b = Batch()
+    kura = open(system_path("kuramoto")).read()
+    no_jac = re.sub(r"void calc_jacobian.*?\n}\n", "", kura, flags=re.S)
+    with pytest.raises(N.SodeclError) as e:
+        b.add_class(None, "ie", neq=4, npar=5, dt=0.01, system_src=no_jac)
+    assert e.value.status == N.ERR_NO_JACOBIAN
+    with pytest.raises(N.SodeclError):
+        b.add_class(system_path("kuramoto"), "rk4", neq=0, npar=1, dt=0.01)
+    with pytest.raises(N.SodeclError):
+        b.add_class(system_path("kuramoto"), "se", neq=4, npar=5, dt=0.01)  # noise without processes
+    for _ in range(32):
+        b.add_class(system_path("kuramoto"), "euler", neq=2, npar=3, dt=0.01)
+    with pytest.raises(N.SodeclError):
+        b.add_class(system_path("kuramoto"), "euler", neq=2, npar=3, dt=0.01)
+    with pytest.raises(N.SodeclError) as e:
+        Batch().set_items([0], [1], [0.0], [0.0], [0.0])
+    assert e.value.status == N.ERR_STATE
+
+
+def single_kernel_final_state(system, solver, neq, npar, nnoi, dt, nsteps, t0, y0, p, counters, gid, fmad):
+    """The same orbit through the single-system kernel, as the tail of a list
+    so its noise stream is keyed by the same global orbit index."""
+    if nsteps == 0:
+        return t0, y0, counters
+    n = gid + 1
+    with Integrator(system_path(system), solver, dt=dt, tspan=nsteps * dt, ksteps=nsteps, neq=neq, npar=npar,
+                    nnoi=nnoi, orbits=n, fmad=fmad) as sim:
+        assert sim.num_chunks == 1
+        sim.upload(np.full(n, t0), np.tile(y0, (n, 1)), np.tile(p, (n, 1)),
+                   np.full(n, counters) if nnoi else None)
+        sim.run(discard=True)
+        t, y, c = sim.state()
+    return t[gid], y[gid], c[gid]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fmad", [False, True])
+def test_batch_matches_single_system_kernel_bit_for_bit(fmad):
+    n = 3000
+    cls, nsteps, t0, y0, p, counters = make_items(n, 1)
+    b = make_batch(fmad)
+    b.set_items(cls, nsteps, t0, y0, p, counters)
+    b.run(graph=False)
+    t, y, cnt, passes, flags = b.results()
+    rng = np.random.default_rng(2)
+    for i in rng.choice(n, 60, replace=False):
+        system, solver, neq, npar, nnoi, dt = CLASSES[cls[i]]
+        tt, yy, cc = single_kernel_final_state(system, solver, neq, npar, nnoi, dt, nsteps[i], t0[i], y0[i], p[i],
+                                               counters[i], i, fmad)
+        np.testing.assert_array_equal(y[i], yy)
+        assert t[i] == tt
+        if nnoi:
+            assert cnt[i] == cc
+    # orbits with no steps come back untouched
+    zero = nsteps == 0
+    assert np.array_equal(t[zero], t0[zero])
+
+
+@pytest.mark.gpu
+def test_batch_graph_replay_continues_from_state():
+    n = 2000
+    cls, nsteps, t0, y0, p, counters = make_items(n, 3)
+    b = make_batch()
+    b.set_items(cls, nsteps, t0, y0, p, counters)
+    b.run(graph=True)
+    b.run(graph=True)  # replay: a second pass from the stored states
+    t2, y2, c2, _, _ = b.results()
+    b2 = make_batch()
+    b2.set_items(cls, 2 * nsteps, t0, y0, p, counters)
+    b2.run(graph=False)
+    t, y, c, _, _ = b2.results()
+    np.testing.assert_array_equal(np.concatenate(y2), np.concatenate(y))
+    np.testing.assert_array_equal(t2, t)
+    np.testing.assert_array_equal(c2, c)
+
+
+@pytest.mark.gpu
+def test_batch_tuner_and_launch_shapes_agree():
+    n = 4000
+    cls, nsteps, t0, y0, p, counters = make_items(n, 4)
+    outs = []
+    for shape in ((64, 0), (256, 1)):
+        b = make_batch()
+        b.set_items(cls, nsteps, t0, y0, p, counters)
+        b.set_launch(*shape)
+        b.run()
+        outs.append(np.concatenate(b.results()[1]))
+    np.testing.assert_array_equal(outs[0], outs[1])
+    b = make_batch()
+    b.set_items(cls, nsteps, t0, y0, p, counters)
+    block, bps, ms = b.tune()
+    assert block in (64, 128, 256) and ms > 0

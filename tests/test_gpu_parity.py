@@ -352,3 +352,56 @@ def test_cpp_sodeclmgr_drop_in(tmp_path):
     assert np.isclose(res, golden).all()
     filemode = np.fromfile(str(tmp_path / "sodecloutput.bin"))
     np.testing.assert_array_equal(filemode, np.fromfile(out_file))
+
+
+# --------------------------------------------------------------------------
+# the reciprocal quotient
+
+
+def test_reciprocal_quotient_equals_ieee_division():
+    bad, a, b = C.c_int64(), C.c_double(), C.c_double()
+    N.check(N.lib.sodecl_cuda_division_check(0, 1 << 33, 20240601, C.byref(bad), C.byref(a), C.byref(b)))
+    assert bad.value == 0, "first differing pair %r / %r" % (a.value, b.value)
+
+
+@pytest.mark.parametrize("fmad", [0, 1])
+@pytest.mark.parametrize("system,solver,dt", [("oculomotor", "rk4", 1e-5), ("oculomotor", "ie", 1e-3),
+                                              ("oculomotor", "euler", 1e-6), ("kuramoto", "se", 0.01)])
+def test_division_modes_give_identical_records(system, solver, dt, fmad):
+    n = 2048
+    if system == "oculomotor":
+        t0, y0, p = oculomotor_inputs(n, 7)
+        kw = dict(neq=6, npar=6)
+        cnt = None
+    else:
+        rng = np.random.default_rng(8)
+        N_osc = 16
+        p = np.concatenate([rng.uniform(0, 5, (n, 1)), np.tile(rng.normal(size=N_osc), (n, 1)),
+                            rng.uniform(0, 0.5, (n, N_osc))], axis=1)
+        t0, y0, cnt = np.zeros(n), rng.uniform(0, 2 * np.pi, (n, N_osc)), np.arange(n) * 4096.0
+        kw = dict(neq=N_osc, npar=2 * N_osc + 1, nnoi=N_osc)
+    kw.update(dt=dt, tspan=400 * dt, ksteps=40, fmad=bool(fmad))
+    out = {}
+    for mode in ("ieee", "reciprocal"):
+        with Integrator(system_path(system), solver, orbits=n, division=mode, **kw) as sim:
+            assert sim.division == mode
+            sim.upload(t0, y0, p, cnt)
+            out[mode] = sim.run()
+    np.testing.assert_array_equal(out["reciprocal"], out["ieee"])
+
+
+def test_autotune_keeps_results():
+    n = 20000
+    t0, y0, p = oculomotor_inputs(n, 9)
+    kw = dict(dt=1e-5, tspan=5e-4, ksteps=10, neq=6, npar=6)
+    with Integrator(system_path("oculomotor"), "rk4", orbits=n, **kw) as sim:
+        sim.upload(t0, y0, p)
+        want = sim.run()
+        sim.upload(t0, y0, p)
+        choice = sim.autotune(sample_orbits=8192, sample_steps=50)
+        assert choice["block"] in (64, 128, 256) and choice["division"] in ("ieee", "reciprocal")
+        assert sim.division == choice["division"]
+        t, y, _ = sim.state()
+        np.testing.assert_array_equal(y, y0)  # tuning ran on copies
+        got = sim.run()
+    np.testing.assert_array_equal(got, want)
