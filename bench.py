@@ -193,8 +193,10 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    n = a.orbits
-    offset = rank * n
+    from sodecl_b200.sharding import max_over_ranks, shard
+
+    # weak scaling: every rank integrates a.orbits orbits of a world x a.orbits job
+    offset, n = shard(a.orbits * world, rank, world)
     t0, y0, p = workload(n, offset)
     tspan = a.nsteps * a.dt
     sim = Integrator(system_path("oculomotor"), a.solver, dt=a.dt, tspan=tspan, ksteps=a.ksteps, neq=6, npar=6,
@@ -244,10 +246,7 @@ def main():
         wall = time.perf_counter() - wall0
     launch_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     ms = float(np.mean(launch_ms))
-    if dist is not None:
-        tmax = torch.tensor([ms], device=dev)
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        ms = float(tmax.item())
+    ms = max_over_ranks(ms, dist, dev)
     rec_last = rec_d[-1].cpu().numpy()
     nan_fraction = float(np.mean(~np.isfinite(rec_last).all(axis=0)))
     value = world * n * a.nsteps / (ms * 1e-3)
@@ -287,10 +286,7 @@ def main():
             e2e_step()
         barrier()
         e2e_s = (time.perf_counter() - w0) / a.steps
-        if dist is not None:
-            tm = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(tm, op=dist.ReduceOp.MAX)
-            e2e_s = float(tm.item())
+        e2e_s = max_over_ranks(e2e_s, dist, dev)
         e2e = {"value": world * n * a.nsteps / e2e_s, "unit": METRIC, "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_s * 1e3, "path": "sodecl_cuda_upload + sodecl_cuda_run, "
                "pinned host buffers"}
@@ -301,6 +297,7 @@ def main():
     if not a.no_extras and rank == 0:
         extras = companions(a, n, dev, stream)
         extras["gradient"] = gradient_companion(dev)
+        extras["uneven_batch"] = batch_companion(dev)
 
     cpu = None
     if rank == 0 and world == 1:
@@ -345,8 +342,9 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
     true_p = NOMINAL * rng.uniform(0.5, 1.5, (n, 6))
     guess = true_p * rng.uniform(0.95, 1.05, (n, 6))
     y0 = np.tile(Y0, (n, 1))
-    kw = dict(dt=dt, tspan=nsteps * dt, ksteps=ksteps, neq=6, npar=6)
+    kw = dict(dt=dt, tspan=(nsteps - 0.5) * dt, ksteps=ksteps, neq=6, npar=6)
     sim = Integrator(system_path("oculomotor"), "rk4", orbits=n, **kw)
+    assert sim.num_chunks * ksteps == nsteps
     T = lambda x: torch.tensor(x, device=dev)  # noqa: E731
     rec = torch.empty((sim.num_records, 6, n), dtype=torch.float64, device=dev)
     td, yd, pd = T(np.zeros(n)), T(y0), T(true_p)
@@ -355,6 +353,7 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
     gen = torch.Generator(device=dev).manual_seed(7)
     targets = rec + 1e-2 * torch.randn(rec.shape, dtype=torch.float64, device=dev, generator=gen)
     adj = Adjoint(sim)
+    adj_tape = Adjoint(sim, use_tape=True)
     wide = Adjoint(Integrator(system_path("oculomotor"), "rk4", orbits=n * 24, **kw))
     t0, y0d, gd = T(np.zeros(n)), T(y0), T(guess)
 
@@ -372,14 +371,93 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
         return float(np.median(out)), r
 
     ms_adj, (loss, gp, gy, flags) = timed(lambda: adj(t0, y0d, gd, targets))
+    ms_tape, (_, gpt, gyt, _) = timed(lambda: adj_tape(t0, y0d, gd, targets), reps=1)
     ms_fd, (fp, fy) = timed(lambda: finite_difference_gradient(t0, y0d, gd, targets, wide))
     ms_fwd, _ = timed(lambda: adj(t0, y0d, gd, targets, with_gradient=False))
     err_p = ((gp - fp).abs().amax(1) / gp.abs().amax(1)).max().item()
     err_y = ((gy - fy).abs().amax(1) / gy.abs().amax(1)).max().item()
+    err_tape = ((gpt - gp).abs().amax(1) / gp.abs().amax(1)).max().item()
     return {"orbits": n, "nsteps": nsteps, "record_every": ksteps, "dt": dt, "adjoint_ms": ms_adj,
+            "adjoint_tape_ms": ms_tape, "rel_diff_tape_vs_analytic": err_tape,
             "finite_difference_ms": ms_fd, "loss_only_ms": ms_fwd, "speedup_vs_fd": ms_fd / ms_adj,
             "rel_diff_params": err_p, "rel_diff_y0": err_y, "tape_overflow": int((flags != 0).sum().item()),
-            "fd": "central, relative step 1e-6, 24 perturbed copies per orbit in one launch"}
+            "fd": "central, relative step 1e-6, 24 perturbed copies per orbit in one launch",
+            "derivatives": "calc_jacobian + calc_jacobian_params of the system file; tape: reverse mode over sode_system"}
+
+
+def batch_companion(dev, n=1 << 13, max_steps=10000, seed=4):
+    """The uneven-sweep shape: orbits mixing Kuramoto N in {4, 16, 64} and the
+    oculomotor model, solver per orbit in {Euler, RK4, implicit Euler}, step
+    counts log-uniform in [10^2, max_steps], FP64.  The full configuration is
+    2^18 orbits and steps up to 10^5; this sample (2^13 orbits, up to 10^4
+    steps) keeps the default run short.  One persistent launch from
+    device work queues (autotuned launch shape, graph replay), against the
+    padded alternative: one launch per class through the single-system kernel,
+    every orbit of a class run for that class's longest step count."""
+    import torch
+
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.batch import Batch
+
+    rng = np.random.default_rng(seed)
+    classes = []
+    for N in (4, 16, 64):
+        for solver in ("euler", "rk4", "ie"):
+            classes.append(("kuramoto", solver, N, N + 1, 0.01))
+    for solver, dt in (("euler", 1e-6), ("rk4", 1e-5), ("ie", 1e-3)):
+        classes.append(("oculomotor", solver, 6, 6, dt))
+    cls = rng.integers(0, len(classes), n).astype(np.int32)
+    steps = np.exp(rng.uniform(np.log(100), np.log(max_steps), n)).astype(np.int64)
+    y0, p = [], []
+    for c in cls:
+        system, solver, neq, npar, dt = classes[c]
+        if system == "oculomotor":
+            y0.append(Y0)
+            p.append(NOMINAL * rng.uniform(0.5, 1.5, 6))
+        else:
+            y0.append(rng.uniform(0, 2 * np.pi, neq))
+            p.append(np.concatenate([[rng.uniform(0, 5)], rng.normal(size=neq)]))
+    b = Batch()
+    for system, solver, neq, npar, dt in classes:
+        b.add_class(system_path(system), solver, neq=neq, npar=npar, dt=dt)
+    b.compile()
+    sample = rng.choice(n, n // 8, replace=False)
+    b.set_items(cls[sample], np.minimum(steps[sample], 200), np.zeros(sample.size), [y0[i] for i in sample],
+                [p[i] for i in sample])
+    block, bps, _ = b.tune()
+    b.set_items(cls, steps, np.zeros(n), y0, p)
+    b.run(graph=True)  # capture
+    times = []
+    for _ in range(2):
+        b.set_items(cls, steps, np.zeros(n), y0, p)
+        b.set_launch(block, bps)
+        times.append(b.run(graph=True))
+    batch_ms = float(np.median(times))
+    useful = int(steps.sum())
+    # padded: per class, every orbit runs the class's longest orbit
+    padded_ms = 0.0
+    stream = torch.cuda.current_stream(dev)
+    for k, (system, solver, neq, npar, dt) in enumerate(classes):
+        idx = np.nonzero(cls == k)[0]
+        if idx.size == 0:
+            continue
+        m = int(steps[idx].max())
+        sim = Integrator(system_path(system), solver, dt=dt, tspan=(m - 0.5) * dt, ksteps=m, neq=neq, npar=npar,
+                         orbits=idx.size)
+        td = torch.zeros(idx.size, dtype=torch.float64, device=dev)
+        yd = torch.tensor(np.stack([y0[i] for i in idx]), device=dev)
+        pd = torch.tensor(np.stack([p[i] for i in idx]), device=dev)
+        s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_.record(stream)
+        sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(), stream=stream.cuda_stream)
+        e_.record(stream)
+        torch.cuda.synchronize()
+        padded_ms += s_.elapsed_time(e_)
+        sim.close()
+    return {"orbits": n, "classes": len(classes), "steps": "log-uniform [100, %d]" % max_steps,
+            "orbit_steps": useful, "batch_ms": batch_ms, "value": useful / (batch_ms * 1e-3), "unit": METRIC,
+            "tuned_launch": {"block": block, "blocks_per_sm": bps}, "padded_per_class_ms": padded_ms,
+            "speedup_vs_padded": padded_ms / batch_ms, "registers": b.kernel_info()["registers"]}
 
 
 def companions(a, n, dev, stream):

@@ -96,6 +96,7 @@ class AdjointIO(C.Structure):
         ("n", C.c_int64),
         ("ckpt_every", C.c_int32),
         ("tape_entries", C.c_int32),
+        ("use_tape", C.c_int32),
     ]
 
 

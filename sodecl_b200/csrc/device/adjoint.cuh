@@ -19,6 +19,11 @@
 // Part 1 (before the user file): the tape and the sodecl_ad type.
 // Part 2 (SODECL_ADJOINT_KERNEL, after both copies of the user file): the
 // step adjoints and the kernel.
+//
+// When the system file provides both calc_jacobian (df/dy, as the implicit
+// solvers use it) and calc_jacobian_params (df/dp), the products come from
+// them instead (SODECL_ADJ_ANALYTIC): no tape, all in registers -- the fast
+// path; the tape serves every other system file.
 
 #ifndef SODECL_ADJOINT_TYPES
 #define SODECL_ADJOINT_TYPES
@@ -168,30 +173,59 @@ __device__ __forceinline__ void sodecl_tape_sweep(const sodecl_tape &t, double *
 // Part 2.  Needs: the plain system (sode_system), the recording copy
 // (sodecl_adsys::sode_system), the solver step functions (solvers.cuh).
 
+#if SODECL_ADJ_ANALYTIC
+// For the seed v: xbar += v^T df/dx, pbar += v^T df/dp, from the system
+// file's own Jacobians (calc_jacobian, calc_jacobian_params): two small
+// dense products, everything in registers.
+__device__ __forceinline__ void sodecl_vjp(double t, const double *x, const double *p, const double *v, double *xbar,
+                                           double *pbar, sodecl_tape *tape, double *adj, int &overflow)
+{
+    (void)t;
+    (void)tape;
+    (void)adj;
+    (void)overflow;
+    real_t xx[_numeq_], pp[SODECL_NPAR_ALLOC];
+    real_t jy[_numeq_][_numeq_], jp[_numeq_][SODECL_NPAR_ALLOC];
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) xx[e] = (real_t)x[e];
+#pragma unroll SODECL_PAR_UNROLL
+    for (int j = 0; j < _numpar_; ++j) pp[j] = (real_t)p[j];
+    calc_jacobian(xx, jy, pp);
+    calc_jacobian_params(xx, jp, pp);
+#pragma unroll SODECL_EQ_UNROLL
+    for (int i = 0; i < _numeq_; ++i) {
+#pragma unroll SODECL_EQ_UNROLL
+        for (int j = 0; j < _numeq_; ++j) xbar[j] += (double)jy[i][j] * v[i];
+#pragma unroll SODECL_PAR_UNROLL
+        for (int j = 0; j < _numpar_; ++j) pbar[j] += (double)jp[i][j] * v[i];
+    }
+}
+#else
 // f(t, x) and, for the seed v, xbar += v^T df/dx, pbar += v^T df/dp.
 __device__ __forceinline__ void sodecl_vjp(double t, const double *x, const double *p, const double *v, double *xbar,
-                                           double *pbar, sodecl_tape &tape, double *adj, int &overflow)
+                                           double *pbar, sodecl_tape *tape, double *adj, int &overflow)
 {
-    tape.n = 0;
-    tape.overflow = 0;
+    tape->n = 0;
+    tape->overflow = 0;
     sodecl_ad xa[_numeq_], pa[SODECL_NPAR_ALLOC], fa[_numeq_];
-    for (int e = 0; e < _numeq_; ++e) xa[e] = sodecl_ad(x[e], sodecl_tape_push(&tape, -1, 0.0, -1, 0.0), &tape);
-    for (int j = 0; j < _numpar_; ++j) pa[j] = sodecl_ad(p[j], sodecl_tape_push(&tape, -1, 0.0, -1, 0.0), &tape);
+    for (int e = 0; e < _numeq_; ++e) xa[e] = sodecl_ad(x[e], sodecl_tape_push(tape, -1, 0.0, -1, 0.0), tape);
+    for (int j = 0; j < _numpar_; ++j) pa[j] = sodecl_ad(p[j], sodecl_tape_push(tape, -1, 0.0, -1, 0.0), tape);
     sodecl_adsys::sode_system(sodecl_ad(t), xa, fa, pa);
-    for (int k = 0; k < tape.n; ++k) adj[k] = 0.0;
+    for (int k = 0; k < tape->n; ++k) adj[k] = 0.0;
     for (int e = 0; e < _numeq_; ++e)
         if (fa[e].id >= 0) adj[fa[e].id] += v[e];
-    sodecl_tape_sweep(tape, adj);
+    sodecl_tape_sweep(*tape, adj);
     for (int e = 0; e < _numeq_; ++e) xbar[e] += adj[e];
     for (int j = 0; j < _numpar_; ++j) pbar[j] += adj[_numeq_ + j];
-    if (tape.overflow) overflow = 1;
+    if (tape->overflow) overflow = 1;
 }
+#endif
 
 // lambda <- (d step / d y)^T lambda, pbar += (d step / d p)^T lambda, for the
 // step taken from (t, y) with step h: the adjoint of sodecl_step_euler /
 // sodecl_step_rk4's arithmetic.
 __device__ __forceinline__ void sodecl_step_adjoint(double h, double t, const double *y, const double *p,
-                                                    double *lambda, double *pbar, sodecl_tape &tape, double *adj,
+                                                    double *lambda, double *pbar, sodecl_tape *tape, double *adj,
                                                     int &overflow)
 {
 #if SODECL_SOLVER == 1
@@ -304,8 +338,14 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX) sodecl_adjoint(co
     if (!a.grad_p) return;
 
     // backward, segment by segment from the last
-    sodecl_tape tape;
+#if SODECL_ADJ_ANALYTIC
+    sodecl_tape *tape = nullptr;  // the analytic products record nothing
+    double *adj = nullptr;
+#else
+    sodecl_tape tape_storage;
     double adj[SODECL_TAPE_CAP];
+    sodecl_tape *tape = &tape_storage;
+#endif
     double lambda[_numeq_], pbar[SODECL_NPAR_ALLOC], pd[SODECL_NPAR_ALLOC];
     for (int e = 0; e < _numeq_; ++e) lambda[e] = 0.0;
     for (int j = 0; j < _numpar_; ++j) { pbar[j] = 0.0; pd[j] = (double)p[j]; }

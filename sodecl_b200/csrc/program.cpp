@@ -337,6 +337,7 @@ SystemTraits inspect_system(const std::string &src)
     t.has_system = defines_function(stripped, "sode_system");
     t.has_jacobian = defines_function(stripped, "calc_jacobian");
     t.has_stoch = defines_function(stripped, "sode_system_stoch");
+    t.has_pjacobian = defines_function(stripped, "calc_jacobian_params");
     t.uses_listsize = std::regex_search(stripped, std::regex("\\b_listsize_\\b"));
     return t;
 }
@@ -504,7 +505,7 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
     return s.str();
 }
 
-std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, int tape_cap)
+std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, int tape_cap, bool analytic)
 {
     const SystemTraits tr = inspect_system(src);
     std::ostringstream s;
@@ -516,6 +517,7 @@ std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, in
     s << "#define SODECL_NEWTON_MAX " << spec.newton_max_iter << "\n";
     s << "#define SODECL_BLOCK_MAX " << spec.block_max << "\n";
     s << "#define SODECL_TAPE_CAP " << tape_cap << "\n";
+    s << "#define SODECL_ADJ_ANALYTIC " << (analytic ? 1 : 0) << "\n";
     s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n" << kAdjointSrc << "\n";
     s << "#define _numnoi_ " << spec.num_noi << "\n";
     s << "#define _listsize_ " << spec.list_size << "\n";
@@ -539,9 +541,10 @@ std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, in
 
 }  // namespace
 
-std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std::string &system_src, int tape_cap)
+std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std::string &system_src, int tape_cap,
+                                             bool analytic)
 {
-    return compile_text(assemble_adjoint(spec, system_src, tape_cap), spec.fmad, false, "sodecl_adjoint");
+    return compile_text(assemble_adjoint(spec, system_src, tape_cap, analytic), spec.fmad, false, "sodecl_adjoint");
 }
 
 std::shared_ptr<const Program> build_batch(const std::vector<BatchClass> &classes, bool fmad, bool fast_div,

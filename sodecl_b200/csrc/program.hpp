@@ -39,6 +39,7 @@ struct SystemTraits {
     bool has_system = false;
     bool has_jacobian = false;
     bool has_stoch = false;
+    bool has_pjacobian = false;  // calc_jacobian_params (df/dp), used by the adjoint
     bool uses_listsize = false;
 };
 
@@ -61,8 +62,10 @@ std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string 
 
 // The discrete-adjoint program (kernel `sodecl_adjoint`) for the Euler or RK4
 // solver: the system file twice, plain and with `double` recording on a tape
-// of `tape_cap` entries per right-hand-side evaluation.
-std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std::string &system_src, int tape_cap);
+// of `tape_cap` entries per right-hand-side evaluation; with `analytic`, the
+// products come from the file's calc_jacobian and calc_jacobian_params.
+std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std::string &system_src, int tape_cap,
+                                             bool analytic);
 
 // One class of a heterogeneous batch: a system file with a solver, sizes,
 // step and Newton settings (kernel_steps/list_size unused).

@@ -101,6 +101,7 @@ struct sodecl_ctx {
     cudaLibrary_t adj_lib = nullptr;
     cudaKernel_t adj_kernel = nullptr;
     int adj_tape = 0;
+    bool adj_analytic = false;
     void *adj_scratch = nullptr;
     size_t adj_scratch_bytes = 0;
 
@@ -733,15 +734,18 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     if (ctx->system_src.empty()) return ctx->fail(SODECL_ERR_STATE, "compile the system first");
     DeviceScope dev(ctx->cfg.device);
     const int tape = io->tape_entries > 0 ? io->tape_entries : 256;
-    if (!ctx->adj_prog || ctx->adj_tape != tape) {
+    const auto traits = sodecl_b200::inspect_system(ctx->system_src);
+    const bool analytic = !io->use_tape && traits.has_jacobian && traits.has_pjacobian;
+    if (!ctx->adj_prog || ctx->adj_tape != tape || ctx->adj_analytic != analytic) {
         try {
             ProgramSpec spec = make_spec(ctx->cfg);
-            auto prog = sodecl_b200::build_adjoint(spec, ctx->system_src, tape);
+            auto prog = sodecl_b200::build_adjoint(spec, ctx->system_src, tape, analytic);
             if (ctx->adj_lib) cudaLibraryUnload(ctx->adj_lib);
             ctx->adj_lib = nullptr;
             ctx->adj_kernel = nullptr;
             ctx->adj_prog = prog;
             ctx->adj_tape = tape;
+            ctx->adj_analytic = analytic;
         } catch (const std::exception &ex) {
             return ctx->fail(SODECL_ERR_COMPILE, ex.what());
         }

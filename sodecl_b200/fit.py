@@ -28,10 +28,13 @@ def _torch():
 
 
 class Adjoint:
-    def __init__(self, integrator, ckpt_every=0, tape_entries=256):
+    def __init__(self, integrator, ckpt_every=0, tape_entries=256, use_tape=False):
+        """use_tape: differentiate sode_system on the reverse-mode tape even if
+        the system file provides calc_jacobian and calc_jacobian_params."""
         self.sim = integrator
         self.ckpt_every = int(ckpt_every)
         self.tape_entries = int(tape_entries)
+        self.use_tape = bool(use_tape)
 
     def __call__(self, t0, y0, params, targets, with_gradient=True):
         """(loss[n], grad_params[n,npar] or None, grad_y0[n,neq] or None, flags[n])
@@ -56,6 +59,7 @@ class Adjoint:
         io.n = n
         io.ckpt_every = self.ckpt_every
         io.tape_entries = self.tape_entries
+        io.use_tape = 1 if self.use_tape else 0
         stream = torch.cuda.current_stream(dev).cuda_stream
         N.check(N.lib.sodecl_cuda_adjoint(self.sim.ctx, C.byref(io), stream), self.sim.ctx)
         return loss, gp, gy, flags

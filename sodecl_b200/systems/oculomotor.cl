@@ -16,7 +16,11 @@
  * Same model and the same floating-point evaluation order as the
  * reference's examples/oculomotor.cl (sburstf :5-20, dsburstf :22-36,
  * calc_jacobian :38-81, sode_system :83-97, sode_system_stoch :99-112),
- * so trajectories agree with the reference to the last bits.
+ * so trajectories agree with the reference to the last bits.  Two
+ * differences, neither of which changes a trajectory: jac[4][5] carries the
+ * chain-rule sign the reference's calc_jacobian omits (entries off the three
+ * bands are never read by the implicit solvers), and calc_jacobian_params
+ * (df/dp, for the adjoint) is an addition.
  */
 
 #define OCM_T1 0.15
@@ -95,10 +99,66 @@ void calc_jacobian(double y[_numeq_], double jac[_numeq_][_numeq_], double p[_nu
 
 	jac[4][3] = -(2 * p[3] * y[4] * y[3]) / p[2];
 	jac[4][4] = -(p[3] * (y[3] * y[3]) + 1) / p[2];
-	jac[4][5] = ocm_burst_slope(-y[5], p[0], p[1], p[4], p[5]) / p[2];
+	/* d/dy5 of ocm_burst(-y5): note the chain-rule sign, which the reference's
+	 * file omits (its banded solve never reads this entry, so the solvers'
+	 * results are the same either way; full-Jacobian users need the sign) */
+	jac[4][5] = -ocm_burst_slope(-y[5], p[0], p[1], p[4], p[5]) / p[2];
 
 	jac[5][3] = -1;
 	jac[5][4] = 1;
+}
+
+/* d(ocm_burst)/d(a, b, at, bt) */
+void ocm_burst_dparams(double x, double a, double b, double at, double bt, double d[4])
+{
+	if (x > 0)
+	{
+		double e = exp(-x / bt);
+		d[0] = 0;
+		d[1] = 0;
+		d[2] = 1.00 - e;
+		d[3] = -(at * x * e) / (bt * bt);
+	}
+	else
+	{
+		double e = exp(x / b);
+		d[0] = -(x * e) / b;
+		d[1] = (a * x * e) / (b * b) * (1.00 + x / b);
+		d[2] = 0;
+		d[3] = 0;
+	}
+}
+
+/* df/dp, jacp[i][k] = d yout[i] / d p[k] for the six model parameters.  Not in
+ * the reference's file: the adjoint (model fitting) uses it together with
+ * calc_jacobian; without it the adjoint differentiates sode_system itself. */
+void calc_jacobian_params(double y[_numeq_], double jacp[_numeq_][_numpar_], double p[_numpar_])
+{
+	int i, k;
+	double dr[4], dl[4];
+	for (i = 0; i < 6; i++)
+	{
+		for (k = 0; k < _numpar_; k++)
+		{
+			jacp[i][k] = 0;
+		}
+	}
+	ocm_burst_dparams(y[5], p[0], p[1], p[4], p[5], dr);
+	ocm_burst_dparams(-y[5], p[0], p[1], p[4], p[5], dl);
+	double r = -y[3] - (p[3] * y[3] * y[4] * y[4]) + ocm_burst(y[5], p[0], p[1], p[4], p[5]);
+	double l = -y[4] - (p[3] * y[4] * y[3] * y[3]) + ocm_burst(-y[5], p[0], p[1], p[4], p[5]);
+	jacp[3][0] = dr[0] / p[2];
+	jacp[3][1] = dr[1] / p[2];
+	jacp[3][2] = -r / (p[2] * p[2]);
+	jacp[3][3] = -(y[3] * y[4] * y[4]) / p[2];
+	jacp[3][4] = dr[2] / p[2];
+	jacp[3][5] = dr[3] / p[2];
+	jacp[4][0] = dl[0] / p[2];
+	jacp[4][1] = dl[1] / p[2];
+	jacp[4][2] = -l / (p[2] * p[2]);
+	jacp[4][3] = -(y[4] * y[3] * y[3]) / p[2];
+	jacp[4][4] = dl[2] / p[2];
+	jacp[4][5] = dl[3] / p[2];
 }
 
 void sode_system_stoch(double t, double y[_numeq_], double stoch[_numeq_], double p[_numpar_], double noise[_numnoi_])
