@@ -285,6 +285,36 @@ int sodecl_batch_results(sodecl_batch *b, double *t, double *y, double *counters
 int sodecl_batch_last_ms(const sodecl_batch *b, double *ms);
 int sodecl_batch_kernel_info(sodecl_batch *b, int *regs, int *local_bytes);
 size_t sodecl_batch_last_error(const sodecl_batch *b, char *buf, size_t n);
+
+/* Allocation-free launch of a compiled batch.  No counterpart in the
+ * reference.  For callers that cannot let a library call cudaMalloc -- a
+ * custom operator inside a framework whose allocator owns all device memory,
+ * or a service that allocates its working set once at start-up -- because an
+ * allocation (or free) in their launch path synchronises the device and
+ * fragments memory they manage.  The caller passes every input and output as
+ * device memory it owns: orbits grouped by class (class 0's first, then
+ * class 1's, ...; counts in the host array class_count, one entry per class),
+ * states and parameters packed in that order with each class's widths.  The
+ * kernel's only scratch, one work-queue head per class, is a 256-byte
+ * file-scope device array inside the library (at most 32 classes; more is
+ * rejected): every GPU that loads the library holds it until exit, every call
+ * on a device shares it, each call clears it on `stream` before its launch,
+ * and calls that overlap on the GPU race on it.  The first call on a device
+ * loads the batch program there and looks up the array's address; make that
+ * first call before any stream capture.  Returns after queuing the launch on
+ * `stream`; the noise stream of an orbit is keyed by its position. */
+typedef struct sodecl_batch_io {
+    double *t;                  /* [n] in/out */
+    double *y;                  /* states, in/out */
+    const double *params;       /* parameters */
+    double *counters;           /* [n] in/out, or NULL when no class is stochastic */
+    const int64_t *nsteps;      /* [n] */
+    int64_t *newton_passes;     /* [n] out, or NULL */
+    int32_t *flags;             /* [n] out, or NULL */
+    const int64_t *class_count; /* host, one count per class */
+} sodecl_batch_io;
+
+int sodecl_batch_run_noalloc(sodecl_batch *b, const sodecl_batch_io *io, void *stream);
 size_t sodecl_batch_program_source(const sodecl_batch *b, char *buf, size_t n);
 void sodecl_batch_destroy(sodecl_batch *b);
 

@@ -102,6 +102,19 @@ class AdjointIO(C.Structure):
 
 FLAG_TAPE_OVERFLOW = 4
 
+
+class BatchIO(C.Structure):
+    _fields_ = [
+        ("t", C.c_void_p),
+        ("y", C.c_void_p),
+        ("params", C.c_void_p),
+        ("counters", C.c_void_p),
+        ("nsteps", C.c_void_p),
+        ("newton_passes", C.c_void_p),
+        ("flags", C.c_void_p),
+        ("class_count", C.c_void_p),
+    ]
+
 _P = C.c_void_p
 # name -> (restype, argtypes); every function include/sodecl_cuda.h declares
 SIGNATURES = {
@@ -145,6 +158,7 @@ SIGNATURES = {
     "sodecl_batch_last_error": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
     "sodecl_batch_program_source": (C.c_size_t, [_P, C.c_char_p, C.c_size_t]),
     "sodecl_batch_destroy": (None, [_P]),
+    "sodecl_batch_run_noalloc": (C.c_int, [_P, C.POINTER(BatchIO), _P]),
     "sodecl_cuda_fma_peak": (C.c_int, [C.c_int, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
 

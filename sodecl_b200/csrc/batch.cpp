@@ -16,76 +16,9 @@
 #include <string>
 #include <vector>
 
+#include "batch_internal.hpp"
 #include "program.hpp"
 #include "sodecl_cuda.h"
-
-namespace {
-
-constexpr int kMaxClasses = 32;
-
-// Must match struct sodecl_batch_args in device/batch.cuh field for field.
-struct BatchArgs {
-    double *t;
-    double *y;
-    const double *p;
-    double *counters;
-    const long long *nsteps;
-    const long long *orbit_id;
-    long long *newton_passes;
-    int *flags;
-    unsigned long long *head;
-    int nclasses;
-    int order[kMaxClasses];
-    long long begin[kMaxClasses];
-    long long end[kMaxClasses];
-    long long ybase[kMaxClasses];
-    long long pbase[kMaxClasses];
-};
-
-struct Class {
-    sodecl_b200::BatchClass def;
-    double cost_per_step = 1.0;  // relative estimate, orders the classes
-};
-
-}  // namespace
-
-struct sodecl_batch {
-    int device = 0;
-    int fmad = 1;
-    int division = SODECL_DIV_RECIPROCAL;
-    int block = 128;
-    int blocks_per_sm = 0;  // 0 = occupancy limit
-    std::vector<Class> classes;
-    std::shared_ptr<const sodecl_b200::Program> prog;
-    cudaLibrary_t lib = nullptr;
-    cudaKernel_t kernel = nullptr;
-    cudaStream_t stream = nullptr;
-    std::string error;
-
-    // items, sorted by (class, descending steps); perm[sorted] = caller index
-    int64_t nitems = 0;
-    std::vector<int64_t> perm;
-    std::vector<int32_t> item_class;
-    std::vector<int64_t> y_off, p_off;  // caller packing offsets
-    BatchArgs args{};
-    double *d_t = nullptr, *d_y = nullptr, *d_p = nullptr, *d_cnt = nullptr;
-    long long *d_nsteps = nullptr, *d_orbit = nullptr, *d_passes = nullptr;
-    int *d_flags = nullptr;
-    unsigned long long *d_head = nullptr;
-    int64_t total_y = 0, total_p = 0;
-    bool has_counters = false;
-
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t graph_exec = nullptr;
-    int graph_grid = 0, graph_block = 0;
-    double last_ms = 0.0;
-
-    int fail(int code, const std::string &m)
-    {
-        error = m;
-        return code;
-    }
-};
 
 namespace {
 
@@ -221,7 +154,7 @@ int sodecl_batch_add_class(sodecl_batch *b, const char *system_src, size_t len, 
         !std::isfinite(c.dt) || (c.solver == SODECL_STOCHASTIC_EULER && c.num_noi < 1) || c.newton_max_iter < 0 ||
         c.newton_tol < 0)
         return b->fail(SODECL_ERR_INVALID_ARG, "invalid class configuration");
-    Class cl;
+    sodecl_b200_batch::Class cl;
     cl.def.system_src.assign(system_src, len);
     const auto traits = sodecl_b200::inspect_system(cl.def.system_src);
     if (!traits.has_system) return b->fail(SODECL_ERR_COMPILE, "the system file defines no sode_system(...)");
@@ -526,6 +459,10 @@ size_t sodecl_batch_program_source(const sodecl_batch *b, char *buf, size_t n)
 void sodecl_batch_destroy(sodecl_batch *b)
 {
     if (!b) return;
+    if (b->noalloc_lib) {
+        Scope scope(b->device);
+        cudaLibraryUnload(b->noalloc_lib);
+    }
     if (b->lib) {
         Scope scope(b->device);
         if (b->stream) cudaStreamSynchronize(b->stream);

@@ -1,0 +1,89 @@
+// Internal to libsodecl_cuda: the batch object and the kernel-argument block
+// of the persistent batch kernel, shared by batch.cpp and batch_noalloc.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "program.hpp"
+#include "sodecl_cuda.h"
+
+namespace sodecl_b200_batch {
+
+constexpr int kMaxClasses = 32;
+
+// Must match struct sodecl_batch_args in device/batch.cuh field for field.
+struct BatchArgs {
+    double *t;
+    double *y;
+    const double *p;
+    double *counters;
+    const long long *nsteps;
+    const long long *orbit_id;
+    long long *newton_passes;
+    int *flags;
+    unsigned long long *head;
+    int nclasses;
+    int order[kMaxClasses];
+    long long begin[kMaxClasses];
+    long long end[kMaxClasses];
+    long long ybase[kMaxClasses];
+    long long pbase[kMaxClasses];
+};
+
+struct Class {
+    sodecl_b200::BatchClass def;
+    double cost_per_step = 1.0;  // relative estimate, orders the classes
+};
+
+}  // namespace sodecl_b200_batch
+
+using sodecl_b200_batch::BatchArgs;
+using sodecl_b200_batch::kMaxClasses;
+
+struct sodecl_batch {
+    int device = 0;
+    int fmad = 1;
+    int division = SODECL_DIV_RECIPROCAL;
+    int block = 128;
+    int blocks_per_sm = 0;  // 0 = occupancy limit
+    std::vector<sodecl_b200_batch::Class> classes;
+    std::shared_ptr<const sodecl_b200::Program> prog;
+    cudaLibrary_t lib = nullptr;
+    cudaKernel_t kernel = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string error;
+
+    // items, sorted by (class, descending steps); perm[sorted] = caller index
+    int64_t nitems = 0;
+    std::vector<int64_t> perm;
+    std::vector<int32_t> item_class;
+    std::vector<int64_t> y_off, p_off;  // caller packing offsets
+    BatchArgs args{};
+    double *d_t = nullptr, *d_y = nullptr, *d_p = nullptr, *d_cnt = nullptr;
+    long long *d_nsteps = nullptr, *d_orbit = nullptr, *d_passes = nullptr;
+    int *d_flags = nullptr;
+    unsigned long long *d_head = nullptr;
+    int64_t total_y = 0, total_p = 0;
+    bool has_counters = false;
+
+    // program loaded by sodecl_batch_run_noalloc when the caller never
+    // uploaded items through sodecl_batch_set_items
+    cudaLibrary_t noalloc_lib = nullptr;
+    cudaKernel_t noalloc_kernel = nullptr;
+
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_grid = 0, graph_block = 0;
+    double last_ms = 0.0;
+
+    int fail(int code, const std::string &m)
+    {
+        error = m;
+        return code;
+    }
+};
+
