@@ -298,6 +298,7 @@ def main():
         extras = companions(a, n, dev, stream)
         extras["gradient"] = gradient_companion(dev)
         extras["uneven_batch"] = batch_companion(dev)
+        extras["stochastic_kuramoto"] = stochastic_kuramoto_companion(dev, stream)
 
     cpu = None
     if rank == 0 and world == 1:
@@ -458,6 +459,57 @@ def batch_companion(dev, n=1 << 13, max_steps=10000, seed=4):
             "orbit_steps": useful, "batch_ms": batch_ms, "value": useful / (batch_ms * 1e-3), "unit": METRIC,
             "tuned_launch": {"block": block, "blocks_per_sm": bps}, "padded_per_class_ms": padded_ms,
             "speedup_vs_padded": padded_ms / batch_ms, "registers": b.kernel_info()["registers"]}
+
+
+def stochastic_kuramoto_companion(dev, stream, n=1 << 18, N=32, nsteps=2000, ksteps=200, seed=3):
+    """Stochastic Kuramoto by Euler-Maruyama: N=32 phases, 2^18 orbits,
+    K ~ U(0,5), omega ~ N(0,1) shared, additive noise sigma ~ U(0,0.5) per
+    orbit, counters orbit * 2^20, dt=0.01, a record every 200 steps, FP64 (and
+    FP32).  2000 of the full configuration's 2x10^4 steps keep the default run
+    short (the rate does not depend on the step count).  One thread per orbit
+    against the tuned launch (lanes per orbit for this 32-equation system)."""
+    import torch
+
+    from sodecl_b200 import Integrator, system_path
+
+    rng = np.random.default_rng(seed)
+    p = np.concatenate([rng.uniform(0, 5, (n, 1)), np.tile(rng.normal(size=N), (n, 1)),
+                        np.repeat(rng.uniform(0, 0.5, (n, 1)), N, axis=1)], axis=1)
+    th0 = rng.uniform(0, 2 * np.pi, (n, N))
+    cnt = np.arange(n) * 2.0 ** 20
+    out = {}
+    for name, prec, lanes, tune in (("one_thread_per_orbit_fp64", "fp64", 1, False), ("tuned_fp64", "fp64", 1, True),
+                                    ("tuned_fp32", "fp32", 1, True)):
+        sim = Integrator(system_path("kuramoto"), "se", dt=0.01, tspan=nsteps * 0.01, ksteps=ksteps, neq=N,
+                         npar=2 * N + 1, nnoi=N, orbits=n, precision=prec, lanes=lanes)
+        choice = None
+        if tune:
+            sim.upload(np.zeros(n), th0, p, cnt)
+            choice = sim.autotune(sample_orbits=1 << 15, sample_steps=100)
+        td, yd, pd, cd = [torch.tensor(x, device=dev) for x in (np.zeros(n), th0, p, cnt)]
+        rec = torch.empty((sim.num_records, N, n), dtype=torch.float64, device=dev)
+        ms = []
+        for it in range(3):
+            td.zero_()
+            yd.copy_(torch.tensor(th0, device=dev))
+            cd.copy_(torch.tensor(cnt, device=dev))
+            s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_.record(stream)
+            sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(), counters=cd.data_ptr(),
+                       records=rec.data_ptr(), stream=stream.cuda_stream)
+            e_.record(stream)
+            torch.cuda.synchronize()
+            if it > 0:
+                ms.append(s_.elapsed_time(e_))
+        info = sim.kernel_info()
+        out[name] = {"value": n * nsteps / (np.mean(ms) * 1e-3), "unit": METRIC, "ms": float(np.mean(ms)),
+                     "precision": prec, "launch": choice or {"lanes": 1, "block": 128},
+                     "registers": info["registers"], "local_bytes": info["local_bytes"]}
+        sim.close()
+        del rec
+        torch.cuda.empty_cache()
+    out["config"] = {"orbits": n, "N": N, "nsteps": nsteps, "full_nsteps": 20000, "dt": 0.01, "record_every": ksteps}
+    return out
 
 
 def companions(a, n, dev, stream):

@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SODECL_CUDA_ABI_VERSION 1
+#define SODECL_CUDA_ABI_VERSION 2
 
 /* status codes */
 #define SODECL_OK 0
@@ -94,6 +94,12 @@ typedef struct sodecl_cfg {
     int32_t min_blocks_per_sm; /* launch-bounds occupancy hint for the compiler; 0 = none */
     int32_t division;        /* FP64 quotients: SODECL_DIV_IEEE (default) or SODECL_DIV_RECIPROCAL;
                                 both give the IEEE-rounded quotient bit for bit */
+    int32_t lanes_per_orbit; /* 0 or 1 (default): one thread per orbit.  2, 4, 8, 16 or 32:
+                                that many lanes of a warp share an orbit, each evaluating
+                                some of its equations (wide systems).  Needs the system
+                                file's sode_system_row (and sode_system_stoch_row for the
+                                stochastic solver); Euler, RK4 and Euler-Maruyama only.
+                                Same results either way.  No counterpart in the reference. */
 } sodecl_cfg;
 
 /* Fills the defaults: Euler, fp64, fmad on, Newton 1e-7 / 1000, device 0,
@@ -227,12 +233,14 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
 int sodecl_cuda_kernel_info(sodecl_ctx *ctx, int *regs, int *local_bytes, int *max_threads);
 
 /* Autotuner: times candidate launch shapes (threads per block, resident-block
- * hints) and FP64 division modes on copies of the first `sample_orbits`
- * uploaded orbits for `sample_steps` steps -- the context's state does not
- * advance -- and rebuilds the program with the fastest.  All candidates give
- * identical results.  Writes the choice (any pointer may be NULL). */
+ * hints, and lanes per orbit when the system file has sode_system_row and the
+ * solver is explicit or stochastic) and FP64 division modes on copies of the
+ * first `sample_orbits` uploaded orbits for `sample_steps` steps -- the
+ * context's state does not advance -- and rebuilds the program with the
+ * fastest.  All candidates give identical results.  Writes the choice (any
+ * pointer may be NULL). */
 int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_steps, int32_t *block,
-                         int32_t *min_blocks, int32_t *division, double *best_ms);
+                         int32_t *min_blocks, int32_t *division, int32_t *lanes, double *best_ms);
 
 /* Division mode the program was actually built with (SODECL_DIV_*): the
  * reciprocal mode falls back to IEEE for system files that need plain double. */
@@ -257,6 +265,10 @@ typedef struct sodecl_class_cfg {
     double dt;               /* step, printed to 6 significant digits like _m_dt_ */
     double newton_tol;       /* default 1e-7 */
     int32_t newton_max_iter; /* default 1000 */
+    int32_t lanes_per_orbit; /* 0 (default): automatic -- several lanes per orbit for classes of
+                                12 or more equations whose system file has the per-row functions
+                                (see sodecl_cfg.lanes_per_orbit), else one; 1: one lane;
+                                2..32, a power of two: that many */
 } sodecl_class_cfg;
 
 void sodecl_class_cfg_init(sodecl_class_cfg *cfg);
@@ -271,7 +283,9 @@ int sodecl_batch_compile(sodecl_batch *b);
 int sodecl_batch_set_items(sodecl_batch *b, int64_t n, const int32_t *item_class, const int64_t *nsteps,
                            const double *t0, const double *y0, const double *params, const double *counters);
 /* Threads per block (32..256, multiple of 32) and resident blocks per SM
- * (0 = as many as fit). */
+ * (0 = as many as fit).  Classes with lanes per orbit use 8 x
+ * (32 / lanes) x (slot) bytes of shared memory per warp; a block size whose
+ * warps need more than 48 KiB in all is rejected. */
 int sodecl_batch_set_launch(sodecl_batch *b, int32_t block, int32_t blocks_per_sm);
 /* Autotuner: times every candidate launch shape on the current items (each
  * trial advances them) and keeps the fastest. */

@@ -48,6 +48,7 @@ class Cfg(C.Structure):
         ("record_f32", C.c_int32),
         ("min_blocks_per_sm", C.c_int32),
         ("division", C.c_int32),
+        ("lanes_per_orbit", C.c_int32),
     ]
 
 
@@ -80,6 +81,7 @@ class ClassCfg(C.Structure):
         ("dt", C.c_double),
         ("newton_tol", C.c_double),
         ("newton_max_iter", C.c_int32),
+        ("lanes_per_orbit", C.c_int32),
     ]
 
 
@@ -138,7 +140,7 @@ SIGNATURES = {
     "sodecl_cuda_program_division": (C.c_int, [C.c_void_p]),
     "sodecl_cuda_adjoint": (C.c_int, [C.c_void_p, C.POINTER(AdjointIO), C.c_void_p]),
     "sodecl_cuda_autotune": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
-                                       C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+                                       C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
     "sodecl_cuda_kernel_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "sodecl_cuda_noise_stream": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_int32, C.c_double,
                                            C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -49,7 +49,7 @@ class Integrator:
 
     def __init__(self, system, solver, *, dt, tspan, ksteps, neq, npar, orbits, nnoi=0, device=0,
                  precision="fp64", fmad=True, newton_tol=1e-7, newton_max_iter=1000, block=0,
-                 record_f32=False, min_blocks=0, division="ieee", system_src=None):
+                 record_f32=False, min_blocks=0, division="ieee", lanes=1, system_src=None):
         cfg = N.Cfg()
         N.lib.sodecl_cfg_init(C.byref(cfg))
         cfg.solver = _solver_id(solver)
@@ -69,6 +69,7 @@ class Integrator:
         cfg.record_f32 = 1 if record_f32 else 0
         cfg.min_blocks_per_sm = int(min_blocks)
         cfg.division = N.DIV_RECIPROCAL if str(division).lower() == "reciprocal" else N.DIV_IEEE
+        cfg.lanes_per_orbit = int(lanes)
         self.cfg = cfg
         self._ctx = C.c_void_p()
         rc = N.lib.sodecl_cuda_create(C.byref(cfg), C.byref(self._ctx))
@@ -117,14 +118,17 @@ class Integrator:
         return "ieee" if N.lib.sodecl_cuda_program_division(self._ctx) == N.DIV_IEEE else "reciprocal"
 
     def autotune(self, sample_orbits=1 << 17, sample_steps=200):
-        """Picks threads per block, the resident-block hint and the division
-        mode by timing them on copies of uploaded orbits; returns the choice."""
-        b, m, d, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
+        """Picks threads per block, the resident-block hint, the division mode
+        and (for system files with sode_system_row) lanes per orbit by timing
+        them on copies of uploaded orbits; returns the choice."""
+        b, m, d, ln, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
         N.check(N.lib.sodecl_cuda_autotune(self._ctx, int(sample_orbits), int(sample_steps), C.byref(b), C.byref(m),
-                                           C.byref(d), C.byref(ms)), self._ctx)
+                                           C.byref(d), C.byref(ln), C.byref(ms)), self._ctx)
         self.cfg.local_group_size, self.cfg.min_blocks_per_sm, self.cfg.division = b.value, m.value, d.value
+        self.cfg.lanes_per_orbit = ln.value
         return {"block": b.value, "min_blocks": m.value,
-                "division": "reciprocal" if d.value == N.DIV_RECIPROCAL else "ieee", "sample_ms": ms.value}
+                "division": "reciprocal" if d.value == N.DIV_RECIPROCAL else "ieee", "lanes": ln.value,
+                "sample_ms": ms.value}
 
     def kernel_info(self):
         regs, local, mt = C.c_int(), C.c_int(), C.c_int()

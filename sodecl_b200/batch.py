@@ -40,11 +40,13 @@ class Batch:
             raise N.SodeclError(rc, _err(self._b))
 
     def add_class(self, system, solver, *, neq, npar, dt, nnoi=0, newton_tol=1e-7, newton_max_iter=1000,
-                  system_src=None):
+                  lanes=0, system_src=None):
+        """lanes: lanes per orbit (0 automatic, 1 one lane, 2..32 a power of two)."""
         cfg = N.ClassCfg()
         N.lib.sodecl_class_cfg_init(C.byref(cfg))
         cfg.solver, cfg.num_equat, cfg.num_params, cfg.num_noi = _solver_id(solver), neq, npar, nnoi
         cfg.dt, cfg.newton_tol, cfg.newton_max_iter = dt, newton_tol, newton_max_iter
+        cfg.lanes_per_orbit = int(lanes)
         if system_src is None:
             with open(system, "rb") as f:
                 system_src = f.read()

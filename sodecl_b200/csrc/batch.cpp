@@ -93,7 +93,7 @@ int grid_size(sodecl_batch *b, int block)
 {
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void *>(b->kernel),
-                                                                  block, 0);
+                                                                  block, sodecl_b200_batch::shared_bytes(b, block));
     if (e != cudaSuccess || per_sm < 1) {
         cudaGetLastError();
         per_sm = 1;
@@ -108,8 +108,8 @@ int launch_once(sodecl_batch *b, int block, int grid)
 {
     BATCH_TRY(b, cudaMemsetAsync(b->d_head, 0, sizeof(unsigned long long) * kMaxClasses, b->stream));
     void *params[] = {&b->args};
-    BATCH_TRY(b, cudaLaunchKernel(reinterpret_cast<const void *>(b->kernel), dim3(grid), dim3(block), params, 0,
-                                  b->stream));
+    BATCH_TRY(b, cudaLaunchKernel(reinterpret_cast<const void *>(b->kernel), dim3(grid), dim3(block), params,
+                                  sodecl_b200_batch::shared_bytes(b, block), b->stream));
     return SODECL_OK;
 }
 
@@ -124,6 +124,7 @@ void sodecl_class_cfg_init(sodecl_class_cfg *c)
     c->solver = SODECL_EULER;
     c->newton_tol = 1e-7;
     c->newton_max_iter = 1000;
+    c->lanes_per_orbit = 0;
 }
 
 int sodecl_batch_create(int device, int fmad, int division, sodecl_batch **out)
@@ -152,7 +153,8 @@ int sodecl_batch_add_class(sodecl_batch *b, const char *system_src, size_t len, 
     const sodecl_class_cfg &c = *cfg;
     if (c.solver < 0 || c.solver > 4 || c.num_equat < 1 || c.num_params < 0 || c.num_noi < 0 || !(c.dt > 0) ||
         !std::isfinite(c.dt) || (c.solver == SODECL_STOCHASTIC_EULER && c.num_noi < 1) || c.newton_max_iter < 0 ||
-        c.newton_tol < 0)
+        c.newton_tol < 0 || c.lanes_per_orbit < 0 || c.lanes_per_orbit > 32 ||
+        (c.lanes_per_orbit & (c.lanes_per_orbit - 1)) != 0)
         return b->fail(SODECL_ERR_INVALID_ARG, "invalid class configuration");
     sodecl_b200_batch::Class cl;
     cl.def.system_src.assign(system_src, len);
@@ -171,6 +173,25 @@ int sodecl_batch_add_class(sodecl_batch *b, const char *system_src, size_t len, 
     s.newton_tol = c.newton_tol > 0 ? c.newton_tol : 1e-7;
     s.newton_max_iter = c.newton_max_iter > 0 ? c.newton_max_iter : 1000;
     s.fmad = b->fmad != 0;
+    // lanes per orbit: the per-row functions this solver needs
+    bool rows = traits.has_row;
+    if (c.solver == SODECL_STOCHASTIC_EULER) rows = rows && traits.has_stoch_row;
+    if (c.solver == SODECL_IMPLICIT_EULER || c.solver == SODECL_IMPLICIT_MIDPOINT) rows = rows && traits.has_jac_band;
+    if (c.lanes_per_orbit > 1 && !rows)
+        return b->fail(SODECL_ERR_UNSUPPORTED, "lanes per orbit need sode_system_row(...) in the system file, and "
+                                               "sode_system_stoch_row(...) for the stochastic solver or "
+                                               "calc_jacobian_band(...) for the implicit ones");
+    s.lanes = 1;
+    if (c.lanes_per_orbit > 1) {
+        s.lanes = c.lanes_per_orbit;
+    } else if (c.lanes_per_orbit == 0 && rows && c.num_equat >= 12) {
+        // about two rows per lane
+        s.lanes = 4;
+        while (s.lanes < 32 && 2 * s.lanes < c.num_equat) s.lanes *= 2;
+    }
+    if (s.lanes > 1 && (32 / s.lanes) * sodecl_b200::lanes_slot_words(s) * sizeof(double) * 2 > sodecl_b200_batch::kSharedCap)
+        return b->fail(SODECL_ERR_UNSUPPORTED, "lanes per orbit: one warp's orbits need more than half of a block's "
+                                               "shared memory");
     cl.cost_per_step = step_cost(s);
     b->classes.push_back(std::move(cl));
     if (class_id) *class_id = static_cast<int32_t>(b->classes.size() - 1);
@@ -188,6 +209,9 @@ int sodecl_batch_compile(sodecl_batch *b)
     } catch (const std::exception &ex) {
         return b->fail(SODECL_ERR_COMPILE, ex.what());
     }
+    b->warp_words = sodecl_b200::batch_warp_words(defs);
+    while (b->block > 32 && sodecl_b200_batch::shared_bytes(b, b->block) > sodecl_b200_batch::kSharedCap)
+        b->block -= 32;
     return SODECL_OK;
 }
 
@@ -311,6 +335,9 @@ int sodecl_batch_set_launch(sodecl_batch *b, int32_t block, int32_t blocks_per_s
     if (!b) return SODECL_ERR_INVALID_ARG;
     if (block < 32 || block > 256 || block % 32 || blocks_per_sm < 0)
         return b->fail(SODECL_ERR_INVALID_ARG, "block must be a multiple of 32 in [32, 256]");
+    if (sodecl_b200_batch::shared_bytes(b, block) > sodecl_b200_batch::kSharedCap)
+        return b->fail(SODECL_ERR_INVALID_ARG, "block too large: its warps' lanes-per-orbit slots exceed 48 KiB of "
+                                               "shared memory");
     if (block != b->block || blocks_per_sm != b->blocks_per_sm) drop_graph(b);
     b->block = block;
     b->blocks_per_sm = blocks_per_sm;
@@ -399,6 +426,7 @@ int sodecl_batch_tune(sodecl_batch *b, int32_t *block, int32_t *blocks_per_sm, d
     double best = 1e300;
     int best_block = b->block, best_bps = b->blocks_per_sm;
     for (const auto &sh : shapes) {
+        if (sodecl_b200_batch::shared_bytes(b, sh[0]) > sodecl_b200_batch::kSharedCap) continue;
         int rc = sodecl_batch_set_launch(b, sh[0], sh[1]);
         if (rc != SODECL_OK) return rc;
         rc = sodecl_batch_run(b, 0);

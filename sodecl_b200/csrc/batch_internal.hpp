@@ -70,6 +70,8 @@ struct sodecl_batch {
     int64_t total_y = 0, total_p = 0;
     bool has_counters = false;
 
+    int warp_words = 0;  // doubles of dynamic shared memory per warp (lanes-per-orbit classes)
+
     // program loaded by sodecl_batch_run_noalloc when the caller never
     // uploaded items through sodecl_batch_set_items
     cudaLibrary_t noalloc_lib = nullptr;
@@ -87,3 +89,14 @@ struct sodecl_batch {
     }
 };
 
+namespace sodecl_b200_batch {
+
+// Dynamic shared memory of one block of the batch kernel, and its cap (the
+// default limit, no opt-in).
+constexpr size_t kSharedCap = 48 * 1024;
+inline size_t shared_bytes(const sodecl_batch *b, int block)
+{
+    return static_cast<size_t>(block / 32) * static_cast<size_t>(b->warp_words) * sizeof(double);
+}
+
+}  // namespace sodecl_b200_batch

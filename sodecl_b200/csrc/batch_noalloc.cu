@@ -150,7 +150,8 @@ extern "C" int sodecl_batch_run_noalloc(sodecl_batch *b, const sodecl_batch_io *
 
     const int block = b->block;
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void *>(kernel), block, 0) !=
+    const size_t shared = sodecl_b200_batch::shared_bytes(b, block);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void *>(kernel), block, shared) !=
             cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
@@ -165,7 +166,7 @@ extern "C" int sodecl_batch_run_noalloc(sodecl_batch *b, const sodecl_batch_io *
     if (e == cudaSuccess) {
         void *params[] = {&a};
         e = cudaLaunchKernel(reinterpret_cast<const void *>(kernel), dim3(std::max(1, sms) * per_sm), dim3(block),
-                             params, 0, s);
+                             params, shared, s);
     }
     if (e != cudaSuccess) {
         cudaGetLastError();

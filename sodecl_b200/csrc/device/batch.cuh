@@ -15,7 +15,12 @@
 // and, when that orbit is done, stores it and takes the next one, so lanes
 // of a warp stay busy although their orbits have different lengths; a warp
 // moves on to the next class when the queue is empty for all its lanes.
-// Big orbits go first, small ones fill the tail.
+// Big orbits go first, small ones fill the tail.  Classes of wide systems
+// can run with several lanes per orbit (SODECL_LANES > 1), each group of
+// lanes taking orbits from the queue as one; their vectors live in the
+// warp's region of dynamic shared memory (SODECL_BATCH_WARP_WORDS doubles per
+// warp, the largest need of any such class), and the kernel joins the warp
+// after each class so that no group's slot overlaps the next class's.
 
 #ifndef SODECL_BATCH_SHARED
 #define SODECL_BATCH_SHARED
@@ -41,9 +46,10 @@ struct sodecl_batch_args {
 #endif
 
 #ifdef SODECL_BATCH_CLASS_BODY
+#if SODECL_LANES == 1
 // Runs class `cls` until its queue is empty for every lane of the warp.
 // Called by all 32 lanes of a warp together.
-__device__ __forceinline__ void sodecl_class_run(const sodecl_batch_args &a, const int cls)
+__device__ __forceinline__ void sodecl_class_run(const sodecl_batch_args &a, const int cls, double *)
 {
     const long long begin = a.begin[cls];
     const unsigned long long count = (unsigned long long)(a.end[cls] - begin);
@@ -104,4 +110,72 @@ __device__ __forceinline__ void sodecl_class_run(const sodecl_batch_args &a, con
         }
     }
 }
+#else  // SODECL_LANES > 1
+// Lanes per orbit (wide systems; the step functions of solvers.cuh): each
+// group of SODECL_LANES lanes takes its own orbits from the class queue, one
+// atomic per orbit, and integrates them with the group's barriers only, so the
+// groups of a warp run orbits of different lengths independently.  The
+// group's slot lies in the warp's shared memory region `warp_smem`.
+__device__ __forceinline__ void sodecl_class_run(const sodecl_batch_args &a, const int cls, double *warp_smem)
+{
+    const int wl = threadIdx.x % 32;
+    const int lane = wl % SODECL_LANES;
+    const unsigned gmask = SODECL_LANES == 32 ? 0xffffffffu
+                                              : ((1u << SODECL_LANES) - 1u) << (wl / SODECL_LANES * SODECL_LANES);
+    const sodecl_lanes_view v = sodecl_lanes_slot(
+        reinterpret_cast<real_t *>(warp_smem) + (wl / SODECL_LANES) * SODECL_SLOT, lane, gmask);
+    const long long begin = a.begin[cls];
+    const unsigned long long count = (unsigned long long)(a.end[cls] - begin);
+    unsigned long long *head = a.head + cls;
+    const long long ybase = a.ybase[cls], pbase = a.pbase[cls];
+#pragma unroll 1
+    for (;;) {
+        unsigned long long k = 0;
+        if (lane == 0) k = atomicAdd(head, 1ULL);
+        k = __shfl_sync(gmask, k, 0, SODECL_LANES);
+        if (k >= count) break;
+        const long long item = begin + (long long)k;
+        real_t yown[SODECL_ROWS];
+#pragma unroll
+        for (int q = 0; q < SODECL_ROWS; ++q) {
+            const int r = lane + q * SODECL_LANES;
+            yown[q] = (real_t)0;
+            if (r < _numeq_) {
+                yown[q] = (real_t)a.y[ybase + (long long)k * _numeq_ + r];
+                v.Y[r] = yown[q];
+            }
+        }
+        for (int j = lane; j < _numpar_; j += SODECL_LANES)
+            v.P[j] = (real_t)__ldg(a.p + pbase + (long long)k * _numpar_ + j);
+        __syncwarp(gmask);
+        real_t t = (real_t)a.t[item];
+        double counter = a.counters ? a.counters[item] : 0.0;
+        const long long left = a.nsteps[item];
+        const sodecl_i64 gid = a.orbit_id ? a.orbit_id[item] : item;
+        sodecl_i64 passes = 0;
+        int capped = 0;
+#pragma unroll 1
+        for (long long s = 0; s < left; ++s) sodecl_lanes_advance(t, yown, v, gid, counter, passes, capped);
+        int nonfinite = 0;
+#pragma unroll
+        for (int q = 0; q < SODECL_ROWS; ++q) {
+            const int r = lane + q * SODECL_LANES;
+            if (r < _numeq_) {
+                if (!isfinite(yown[q])) nonfinite = 1;
+                a.y[ybase + (long long)k * _numeq_ + r] = (double)yown[q];
+            }
+        }
+#pragma unroll
+        for (int o = SODECL_LANES / 2; o > 0; o >>= 1) nonfinite |= __shfl_xor_sync(gmask, nonfinite, o, SODECL_LANES);
+        if (lane == 0) {
+            a.t[item] = (double)t;
+            if (a.counters) a.counters[item] = counter;
+            if (a.newton_passes) a.newton_passes[item] = passes;
+            if (a.flags)
+                a.flags[item] = (capped ? SODECL_FLAG_NEWTON_CAP : 0) | (nonfinite ? SODECL_FLAG_NONFINITE : 0);
+        }
+        __syncwarp(gmask);  // the slot is reused by the group's next orbit
+    }
+}
+#endif  // SODECL_LANES
 #endif

@@ -21,9 +21,18 @@
 //   SODECL_HAS_STOCH     the system file defines sode_system_stoch
 //   SODECL_NEWTON_MAX    Newton pass limit (reference: 1000)
 //   SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS   launch bounds
+//   SODECL_LANES         lanes per orbit: 1 (one thread per orbit, the
+//                        default) or 2..32, a power of two (wide systems;
+//                        see the kernel at the end of this file)
+//   SODECL_HAS_ROW, SODECL_HAS_STOCH_ROW, SODECL_HAS_JAC_BAND  the system
+//                        file defines sode_system_row / sode_system_stoch_row /
+//                        calc_jacobian_band
 
 #ifndef SODECL_MIN_BLOCKS
 #define SODECL_MIN_BLOCKS 1
+#endif
+#ifndef SODECL_LANES
+#define SODECL_LANES 1
 #endif
 
 #if SODECL_RECORD_F32
@@ -264,6 +273,322 @@ __device__ __forceinline__ void sodecl_advance(real_t &t, real_t *y, real_t *p, 
     for (int e = 0; e < _numeq_; ++e) y[e] = ynew[e];
 }
 
+#if SODECL_LANES > 1
+// ---------------------------------------------------------------------------
+// Lanes per orbit, for wide systems.  With one thread per orbit, a system of
+// dozens of equations keeps its state and stage vectors in local memory, and
+// every right-hand-side term goes through it.  Here SODECL_LANES consecutive
+// lanes of a warp share one orbit: lane l owns the rows l, l + L, l + 2L, ...
+// and evaluates them with the system file's per-row functions --
+// `sode_system_row(i, t, y, p)` (= yout[i] of sode_system),
+// `sode_system_stoch_row(i, t, y, p, noise)` and, for the implicit solvers,
+// `calc_jacobian_band(i, y, band, p)` (band = row i's entries in columns
+// i-1, i, i+1 of calc_jacobian) -- against the orbit's vectors staged in
+// shared memory, where the lanes of a group read the same word (a broadcast).
+// Every row sees the single-thread solver's arithmetic, and sums over rows
+// (the Newton residual norm) are taken in the same order, gathered with warp
+// shuffles, so results are the same as one thread per orbit.  Noise pairs are
+// drawn by the lanes in turn with the counter values the single thread uses;
+// the banded solve, a sequential recurrence, runs on the group's first lane.
+#if SODECL_LANES > 32 || (SODECL_LANES & (SODECL_LANES - 1)) != 0
+#error "SODECL_LANES must be a power of two up to 32"
+#endif
+#if !SODECL_HAS_ROW
+#error "lanes per orbit need sode_system_row in the system file"
+#endif
+#if SODECL_SOLVER == 0 && !SODECL_HAS_STOCH_ROW
+#error "lanes per orbit with the stochastic solver need sode_system_stoch_row in the system file"
+#endif
+#if (SODECL_SOLVER == 3 || SODECL_SOLVER == 4) && !SODECL_HAS_JAC_BAND
+#error "lanes per orbit with an implicit solver need calc_jacobian_band in the system file"
+#endif
+
+#undef SODECL_ROWS
+#undef SODECL_NPAIRS
+#undef SODECL_LANES_NVEC
+#undef SODECL_SLOT_RAW
+#undef SODECL_SLOT
+#define SODECL_ROWS ((_numeq_ + SODECL_LANES - 1) / SODECL_LANES)
+#define SODECL_NPAIRS ((_numnoi_ + 1) / 2)
+// One orbit's shared slot, in real_t words: SODECL_LANES_NVEC vectors of
+// _numeq_ (state; RK4: two probes; Newton: iterate, midpoint, diagonal,
+// super- and sub-diagonal, right-hand side, update), the parameters and the
+// noise, padded to an odd length so that groups of a warp reading word j of
+// their slots hit different banks.
+#if SODECL_SOLVER == 2
+#define SODECL_LANES_NVEC 3
+#elif SODECL_SOLVER == 3 || SODECL_SOLVER == 4
+#define SODECL_LANES_NVEC 8
+#else
+#define SODECL_LANES_NVEC 1
+#endif
+#define SODECL_SLOT_RAW (SODECL_LANES_NVEC * (_numeq_) + (_numpar_) + (_numnoi_))
+#define SODECL_SLOT ((SODECL_SLOT_RAW) | 1)
+
+struct sodecl_lanes_view {
+    real_t *Y;       // state
+    real_t *A, *B;   // RK4: probes; Newton: iterate x, midpoint
+    real_t *D, *UP, *LO, *V, *DX;  // Newton: the banded system and its solution
+    real_t *P;       // parameters
+    real_t *NZ;      // noise of the step
+    int lane;        // lane within the group
+    unsigned mask;   // lanes taking part in the group's barriers and shuffles
+};
+
+__device__ __forceinline__ sodecl_lanes_view sodecl_lanes_slot(real_t *slot, int lane, unsigned mask)
+{
+    sodecl_lanes_view v;
+    v.Y = slot;
+    v.A = slot + (SODECL_LANES_NVEC > 1 ? 1 : 0) * _numeq_;
+    v.B = slot + (SODECL_LANES_NVEC > 2 ? 2 : 0) * _numeq_;
+    v.D = slot + (SODECL_LANES_NVEC > 3 ? 3 : 0) * _numeq_;
+    v.UP = slot + (SODECL_LANES_NVEC > 4 ? 4 : 0) * _numeq_;
+    v.LO = slot + (SODECL_LANES_NVEC > 5 ? 5 : 0) * _numeq_;
+    v.V = slot + (SODECL_LANES_NVEC > 6 ? 6 : 0) * _numeq_;
+    v.DX = slot + (SODECL_LANES_NVEC > 7 ? 7 : 0) * _numeq_;
+    v.P = slot + SODECL_LANES_NVEC * _numeq_;
+    v.NZ = v.P + _numpar_;
+    v.lane = lane;
+    v.mask = mask;
+    return v;
+}
+
+__device__ __forceinline__ double sodecl_shfl(unsigned m, double x, int src) { return __shfl_sync(m, x, src, SODECL_LANES); }
+__device__ __forceinline__ float sodecl_shfl(unsigned m, float x, int src) { return __shfl_sync(m, x, src, SODECL_LANES); }
+#if SODECL_FAST_DIV
+__device__ __forceinline__ sodecl_f64 sodecl_shfl(unsigned m, sodecl_f64 x, int src)
+{
+    return sodecl_f64(__shfl_sync(m, x.v, src, SODECL_LANES));
+}
+#endif
+
+// The counter after c increments of 1.0, as c sequential additions give it:
+// one addition when the counter is an integer and every partial sum stays
+// within +-2^53 (all exact), else the additions themselves.
+__device__ __forceinline__ double sodecl_counter_plus(double counter, int c)
+{
+    if (counter == floor(counter) && counter >= -9007199254740992.0 && counter <= 9007199254740992.0 - (double)c)
+        return counter + (double)c;
+    double cc = counter;
+    for (int q = 0; q < c; ++q) cc = cc + 1.0;
+    return cc;
+}
+
+#if SODECL_SOLVER == 3 || SODECL_SOLVER == 4
+// sodecl_band_solve on the shared band system (D, UP, LO, V) -> DX, by one lane.
+__device__ __forceinline__ void sodecl_lanes_band_solve(const sodecl_lanes_view &v)
+{
+    real_t dprev = v.D[0], vprev = v.V[0];
+#pragma unroll 1
+    for (int i = 1; i < _numeq_; ++i) {
+        const real_t up = (i < _numeq_ - 2) ? v.UP[i] : (real_t)0;
+        const real_t f = sodecl_qdiv(up, dprev);
+        const real_t lo = v.LO[i - 1];
+        dprev = v.D[i] - f * lo;
+        vprev = v.V[i] - f * vprev;
+        v.D[i] = dprev;
+        v.V[i] = vprev;
+    }
+    real_t x = sodecl_qdiv(v.V[_numeq_ - 1], v.D[_numeq_ - 1]);
+    v.DX[_numeq_ - 1] = x;
+#pragma unroll 1
+    for (int i = _numeq_ - 2; i >= 0; --i) {
+        x = sodecl_qdiv(v.V[i] - v.LO[i] * x, v.D[i]);
+        v.DX[i] = x;
+    }
+}
+
+// sodecl_step_newton, row by row (src/kernels/ie.cl:50-117, im.cl:43-118).
+__device__ __forceinline__ int sodecl_lanes_newton(real_t h, real_t t, const real_t *yown, real_t *xnew,
+                                                   const sodecl_lanes_view &v, int &capped)
+{
+    real_t x[SODECL_ROWS], r[SODECL_ROWS];
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int row = v.lane + k * SODECL_LANES;
+        x[k] = (real_t)0;
+        r[k] = (real_t)0;
+        if (row < _numeq_) {
+            x[k] = yown[k];
+            v.A[row] = x[k];
+        }
+    }
+    __syncwarp(v.mask);
+    int pass = 0;
+    bool done = false;
+#pragma unroll 1
+    for (pass = 0; pass < SODECL_NEWTON_MAX; ++pass) {
+#if SODECL_SOLVER == 4
+        real_t *at = v.B;
+#pragma unroll
+        for (int k = 0; k < SODECL_ROWS; ++k) {
+            const int row = v.lane + k * SODECL_LANES;
+            if (row < _numeq_) v.B[row] = (yown[k] + x[k]) * (real_t)0.5;
+        }
+        __syncwarp(v.mask);
+#else
+        real_t *at = v.A;
+#endif
+#pragma unroll
+        for (int k = 0; k < SODECL_ROWS; ++k) {
+            const int row = v.lane + k * SODECL_LANES;
+            if (row < _numeq_) r[k] = x[k] - yown[k] - sode_system_row(row, t, at, v.P) * h;
+        }
+        // the residual norm in row order, every lane of the group the same
+        real_t norm = 0;
+#pragma unroll
+        for (int e = 0; e < _numeq_; ++e) {
+            const real_t re = sodecl_shfl(v.mask, r[e / SODECL_LANES], e % SODECL_LANES);
+#if SODECL_SOLVER == 4
+            norm = norm + re * re;
+#else
+            norm = norm + fabs(re);
+#endif
+        }
+#if SODECL_SOLVER == 4
+        if (sqrt(norm) < (real_t)_epsilon1_) { done = true; break; }
+        const real_t scale = (real_t)(-0.50);
+#else
+        if (norm < (real_t)_epsilon1_) { done = true; break; }
+        const real_t scale = (real_t)(-1.00);
+#endif
+#pragma unroll
+        for (int k = 0; k < SODECL_ROWS; ++k) {
+            const int row = v.lane + k * SODECL_LANES;
+            if (row < _numeq_) {
+                real_t band[3];
+                calc_jacobian_band(row, at, band, v.P);
+                real_t d = band[1] * scale * h;
+                d = d + 1;
+                v.D[row] = d;
+                if (row < _numeq_ - 2) v.UP[row] = band[2] * scale * h;
+                if (row > 0) v.LO[row - 1] = band[0] * scale * h;
+                v.V[row] = r[k];
+            }
+        }
+        __syncwarp(v.mask);
+        if (v.lane == 0) sodecl_lanes_band_solve(v);
+        __syncwarp(v.mask);
+#pragma unroll
+        for (int k = 0; k < SODECL_ROWS; ++k) {
+            const int row = v.lane + k * SODECL_LANES;
+            if (row < _numeq_) {
+                x[k] = x[k] - v.DX[row];
+                v.A[row] = x[k];
+            }
+        }
+        __syncwarp(v.mask);
+    }
+    if (!done) capped = 1;
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) xnew[k] = x[k];
+    return done ? pass + 1 : pass;
+}
+#endif
+
+// One step of the configured solver for the group's orbit: every lane of the
+// group (all of v.mask) calls it together.
+__device__ __forceinline__ void sodecl_lanes_advance(real_t &t, real_t *yown, const sodecl_lanes_view &v, sodecl_i64 gid,
+                                                     double &counter, sodecl_i64 &passes, int &capped)
+{
+    const real_t h = _m_dt_;
+    real_t ynew[SODECL_ROWS];
+#if SODECL_SOLVER == 1
+    // src/kernels/euler.cl:10-18, row by row
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int r = v.lane + k * SODECL_LANES;
+        if (r < _numeq_) ynew[k] = yown[k] + sode_system_row(r, t, v.Y, v.P) * h;
+    }
+#elif SODECL_SOLVER == 2
+    // src/kernels/rk4.cl:17-64, row by row; the probe alternates between two
+    // buffers so that one barrier per stage suffices
+    real_t stage[SODECL_ROWS];
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int r = v.lane + k * SODECL_LANES;
+        if (r < _numeq_) {
+            ynew[k] = sode_system_row(r, t, v.Y, v.P);
+            stage[k] = ynew[k];
+            v.A[r] = yown[k] + (h * (real_t)0.50) * stage[k];
+        }
+    }
+    __syncwarp(v.mask);
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int r = v.lane + k * SODECL_LANES;
+        if (r < _numeq_) {
+            stage[k] = sode_system_row(r, t + (real_t)0.50 * h, v.A, v.P);
+            ynew[k] = ynew[k] + (real_t)2.00 * stage[k];
+            v.B[r] = yown[k] + (h * (real_t)0.50) * stage[k];
+        }
+    }
+    __syncwarp(v.mask);
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int r = v.lane + k * SODECL_LANES;
+        if (r < _numeq_) {
+            stage[k] = sode_system_row(r, t + (real_t)0.50 * h, v.B, v.P);
+            ynew[k] = ynew[k] + (real_t)2.00 * stage[k];
+            v.A[r] = yown[k] + h * stage[k];
+        }
+    }
+    __syncwarp(v.mask);
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int r = v.lane + k * SODECL_LANES;
+        if (r < _numeq_) {
+            stage[k] = sode_system_row(r, t + h, v.A, v.P);
+            ynew[k] = yown[k] + (ynew[k] + stage[k]) * h / (real_t)6.00;
+        }
+    }
+#elif SODECL_SOLVER == 3 || SODECL_SOLVER == 4
+    passes += sodecl_lanes_newton(h, t, yown, ynew, v, capped);
+#elif SODECL_SOLVER == 0
+    // stochastic_solver_caller.cl:31-66: pair c of this step uses the counter
+    // advanced c times; the lanes draw the pairs in turn
+    const real_t sqrt_h = sqrt((real_t)_m_dt_);
+#pragma unroll 1
+    for (int c = v.lane; c < SODECL_NPAIRS; c += SODECL_LANES) {
+        sodecl_u64 w0, w1;
+        sodecl_threefry2x64_20((sodecl_u64)gid, sodecl_counter_word(sodecl_counter_plus(counter, c)), SODECL_TF_KEY0,
+                               SODECL_TF_KEY1, w0, w1);
+        real_t n0, n1;
+        sodecl_gaussian_pair<real_t>(w0, w1, sqrt_h, n0, n1);
+        v.NZ[2 * c] = n0;
+        if (2 * c + 1 < _numnoi_) v.NZ[2 * c + 1] = n1;
+    }
+    counter = sodecl_counter_plus(counter, SODECL_NPAIRS);
+    __syncwarp(v.mask);
+    // stochastic_euler.cl:10-22, row by row
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int r = v.lane + k * SODECL_LANES;
+        if (r < _numeq_) {
+            const real_t f = sode_system_row(r, t, v.Y, v.P);
+            const real_t g = sode_system_stoch_row(r, t, v.Y, v.P, v.NZ);
+            ynew[k] = yown[k] + f * h + g;
+        }
+    }
+#endif
+    (void)gid;
+    (void)counter;
+    (void)passes;
+    (void)capped;
+    t = t + _m_dt_;
+    __syncwarp(v.mask);  // the group is done reading the state, probes and noise
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int r = v.lane + k * SODECL_LANES;
+        if (r < _numeq_) {
+            yown[k] = ynew[k];
+            v.Y[r] = ynew[k];
+        }
+    }
+    __syncwarp(v.mask);
+}
+#endif  // SODECL_LANES > 1
+
 #ifndef SODECL_STEPS_ONLY
 __device__ __forceinline__ void sodecl_store_record(const sodecl_args &a, int rec, sodecl_i64 i, const real_t *y, int &flags)
 {
@@ -277,6 +602,7 @@ __device__ __forceinline__ void sodecl_store_record(const sodecl_args &a, int re
     if (!finite) flags |= SODECL_FLAG_NONFINITE;
 }
 
+#if SODECL_LANES == 1
 extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS)
 sodecl_orbits(const sodecl_args a)
 {
@@ -322,4 +648,90 @@ sodecl_orbits(const sodecl_args a)
     if (a.newton_passes) a.newton_passes[i] += passes;
     if (a.flags && flags) a.flags[i] |= flags;
 }
+#else  // SODECL_LANES > 1
+__device__ __forceinline__ void sodecl_lanes_store(const sodecl_args &a, int rec, sodecl_i64 i, const real_t *yown,
+                                                   int lane, int &flags)
+{
+    sodecl_record_t *col = a.records + (sodecl_i64)(rec - a.rec_first) * _numeq_ * a.rec_stride + a.rec_col0 + i;
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int r = lane + k * SODECL_LANES;
+        if (r < _numeq_) {
+            finite = finite && isfinite(yown[k]);
+            __stcs(col + (sodecl_i64)r * a.rec_stride, (sodecl_record_t)yown[k]);
+        }
+    }
+    if (!finite) flags |= SODECL_FLAG_NONFINITE;
+}
+
+// Launch: blockDim.x a multiple of 32, grid * blockDim.x >= n * SODECL_LANES,
+// dynamic shared memory blockDim.x / SODECL_LANES * SODECL_SLOT words.  The
+// groups past the last orbit shadow it (all lanes of a group run to the end)
+// and store nothing.
+extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS)
+sodecl_orbits(const sodecl_args a)
+{
+    extern __shared__ __align__(16) unsigned char sodecl_smem[];
+    const int lane = threadIdx.x % SODECL_LANES;
+    // the group's own lanes: groups of a warp leave a Newton iteration after
+    // different numbers of passes, so no barrier or shuffle names another group
+    const unsigned gmask = SODECL_LANES == 32 ? 0xffffffffu
+                                              : ((1u << SODECL_LANES) - 1u) << ((threadIdx.x % 32) / SODECL_LANES * SODECL_LANES);
+    const sodecl_lanes_view v = sodecl_lanes_slot(
+        reinterpret_cast<real_t *>(sodecl_smem) + (threadIdx.x / SODECL_LANES) * SODECL_SLOT, lane, gmask);
+    const sodecl_i64 orbit = ((sodecl_i64)blockIdx.x * blockDim.x + threadIdx.x) / SODECL_LANES;
+    const bool live = orbit < a.n;
+    const sodecl_i64 i = live ? orbit : a.n - 1;
+
+    real_t yown[SODECL_ROWS];
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int r = lane + k * SODECL_LANES;
+        yown[k] = (real_t)0;
+        if (r < _numeq_) {
+            yown[k] = (real_t)a.y[i * _numeq_ + r];
+            v.Y[r] = yown[k];
+        }
+    }
+    for (int k = lane; k < _numpar_; k += SODECL_LANES) v.P[k] = (real_t)__ldg(a.p + i * _numpar_ + k);
+    __syncwarp(gmask);
+    real_t t = (real_t)a.t[i];
+    int flags = 0, capped = 0;
+    sodecl_i64 passes = 0;
+    const sodecl_i64 gid = a.orbit_offset + i;
+#if SODECL_SOLVER == 0
+    double counter = a.counters[i];
+#else
+    double counter = 0.0;
+#endif
+
+#pragma unroll 1
+    for (int c = a.chunk_begin; c < a.chunk_end; ++c) {
+        if (a.records && live) sodecl_lanes_store(a, c, i, yown, lane, flags);
+#pragma unroll 1
+        for (int s = 0; s < _numsteps_; ++s)
+            sodecl_lanes_advance(t, yown, v, gid, counter, passes, capped);
+    }
+    if (a.write_final && a.records && live) sodecl_lanes_store(a, a.chunk_end, i, yown, lane, flags);
+
+#pragma unroll
+    for (int o = SODECL_LANES / 2; o > 0; o >>= 1) flags |= __shfl_xor_sync(gmask, flags, o, SODECL_LANES);
+    if (!live) return;
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int r = lane + k * SODECL_LANES;
+        if (r < _numeq_) a.y[i * _numeq_ + r] = (double)yown[k];
+    }
+    if (lane == 0) {
+        a.t[i] = (double)t;
+#if SODECL_SOLVER == 0
+        a.counters[i] = counter;
+#endif
+        if (capped) flags |= SODECL_FLAG_NEWTON_CAP;
+        if (a.newton_passes) a.newton_passes[i] += passes;
+        if (a.flags && flags) a.flags[i] |= flags;
+    }
+}
+#endif  // SODECL_LANES
 #endif  // SODECL_STEPS_ONLY

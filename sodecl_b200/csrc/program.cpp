@@ -338,8 +338,17 @@ SystemTraits inspect_system(const std::string &src)
     t.has_jacobian = defines_function(stripped, "calc_jacobian");
     t.has_stoch = defines_function(stripped, "sode_system_stoch");
     t.has_pjacobian = defines_function(stripped, "calc_jacobian_params");
+    t.has_row = defines_function(stripped, "sode_system_row");
+    t.has_stoch_row = defines_function(stripped, "sode_system_stoch_row");
+    t.has_jac_band = defines_function(stripped, "calc_jacobian_band");
     t.uses_listsize = std::regex_search(stripped, std::regex("\\b_listsize_\\b"));
     return t;
+}
+
+int lanes_slot_words(const ProgramSpec &spec)
+{
+    const int nvec = spec.solver == 2 ? 3 : (spec.solver == 3 || spec.solver == 4) ? 8 : 1;
+    return (nvec * spec.num_equat + spec.num_params + spec.num_noi) | 1;
 }
 
 std::string assemble(const ProgramSpec &spec, const std::string &system_src, const SystemTraits &traits)
@@ -355,6 +364,10 @@ std::string assemble(const ProgramSpec &spec, const std::string &system_src, con
     s << "#define SODECL_NEWTON_MAX " << spec.newton_max_iter << "\n";
     s << "#define SODECL_BLOCK_MAX " << spec.block_max << "\n";
     if (spec.min_blocks > 0) s << "#define SODECL_MIN_BLOCKS " << spec.min_blocks << "\n";
+    s << "#define SODECL_LANES " << spec.lanes << "\n";
+    s << "#define SODECL_HAS_ROW " << (traits.has_row ? 1 : 0) << "\n";
+    s << "#define SODECL_HAS_STOCH_ROW " << (traits.has_stoch_row ? 1 : 0) << "\n";
+    s << "#define SODECL_HAS_JAC_BAND " << (traits.has_jac_band ? 1 : 0) << "\n";
     s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n";
     // the reference's program defines (src/sodeclmgr.cpp:379-430); _listsize_
     // only when the system file names it, so one program serves every size
@@ -460,6 +473,18 @@ std::vector<std::string> defined_macros(const std::string &src)
     return names;
 }
 
+}  // namespace
+
+int batch_warp_words(const std::vector<BatchClass> &classes)
+{
+    int words = 0;
+    for (const auto &c : classes)
+        if (c.spec.lanes > 1) words = std::max(words, (32 / c.spec.lanes) * lanes_slot_words(c.spec));
+    return words;
+}
+
+namespace {
+
 std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div, int block_max)
 {
     std::ostringstream s;
@@ -470,7 +495,8 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
     s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n" << kBatchSrc << "\n";
     static const char *per_class[] = {"SODECL_SOLVER", "SODECL_HAS_JACOBIAN", "SODECL_HAS_STOCH", "SODECL_NEWTON_MAX",
                                       "_numnoi_", "_numsteps_", "_m_dt_", "_numeq_", "_numpar_", "_epsilon1_",
-                                      "_listsize_", "SODECL_BATCH_CLASS_BODY"};
+                                      "_listsize_", "SODECL_BATCH_CLASS_BODY", "SODECL_LANES", "SODECL_HAS_ROW",
+                                      "SODECL_HAS_STOCH_ROW", "SODECL_HAS_JAC_BAND"};
     for (size_t k = 0; k < classes.size(); ++k) {
         const ProgramSpec &sp = classes[k].spec;
         const std::string &src = classes[k].system_src;
@@ -481,6 +507,10 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
         s << "#define SODECL_HAS_JACOBIAN " << (tr.has_jacobian ? 1 : 0) << "\n";
         s << "#define SODECL_HAS_STOCH " << (tr.has_stoch ? 1 : 0) << "\n";
         s << "#define SODECL_NEWTON_MAX " << sp.newton_max_iter << "\n";
+        s << "#define SODECL_LANES " << sp.lanes << "\n";
+        s << "#define SODECL_HAS_ROW " << (tr.has_row ? 1 : 0) << "\n";
+        s << "#define SODECL_HAS_STOCH_ROW " << (tr.has_stoch_row ? 1 : 0) << "\n";
+        s << "#define SODECL_HAS_JAC_BAND " << (tr.has_jac_band ? 1 : 0) << "\n";
         s << "#define _numnoi_ " << sp.num_noi << "\n";
         s << "#define _listsize_ " << sp.list_size << "\n";
         s << "#define _numsteps_ 1\n";
@@ -497,11 +527,20 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
         s << "#define SODECL_BATCH_CLASS_BODY 1\n#line 1 \"batch.cuh\"\n" << kBatchSrc << "\n";
         s << "}  // namespace sodecl_cls_" << k << "\n";
     }
-    s << "\nextern \"C\" __global__ void __launch_bounds__(SODECL_BLOCK_MAX) sodecl_batch(const sodecl_batch_args a)\n{\n";
+    const int warp_words = batch_warp_words(classes);
+    s << "\n#define SODECL_BATCH_WARP_WORDS " << warp_words << "\n";
+    s << "extern \"C\" __global__ void __launch_bounds__(SODECL_BLOCK_MAX) sodecl_batch(const sodecl_batch_args a)\n{\n";
+    if (warp_words > 0) {
+        s << "    extern __shared__ __align__(16) unsigned char sodecl_smem[];\n";
+        s << "    double *warp_smem = reinterpret_cast<double *>(sodecl_smem) + (threadIdx.x / 32) * "
+             "SODECL_BATCH_WARP_WORDS;\n";
+    } else {
+        s << "    double *warp_smem = nullptr;\n";
+    }
     s << "    for (int k = 0; k < a.nclasses; ++k) {\n        switch (a.order[k]) {\n";
     for (size_t k = 0; k < classes.size(); ++k)
-        s << "        case " << k << ": sodecl_cls_" << k << "::sodecl_class_run(a, " << k << "); break;\n";
-    s << "        default: break;\n        }\n    }\n}\n";
+        s << "        case " << k << ": sodecl_cls_" << k << "::sodecl_class_run(a, " << k << ", warp_smem); break;\n";
+    s << "        default: break;\n        }\n        __syncwarp();\n    }\n}\n";
     return s.str();
 }
 

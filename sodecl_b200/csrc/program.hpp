@@ -24,6 +24,7 @@ struct ProgramSpec {
     int newton_max_iter = 1000;
     int block_max = 256;
     int min_blocks = 0;
+    int lanes = 1;           // lanes per orbit (1, or a power of two up to 32)
 };
 
 struct Program {
@@ -40,6 +41,9 @@ struct SystemTraits {
     bool has_jacobian = false;
     bool has_stoch = false;
     bool has_pjacobian = false;  // calc_jacobian_params (df/dp), used by the adjoint
+    bool has_row = false;        // sode_system_row (one equation's right-hand side)
+    bool has_stoch_row = false;  // sode_system_stoch_row
+    bool has_jac_band = false;   // calc_jacobian_band (row i's entries in columns i-1, i, i+1)
     bool uses_listsize = false;
 };
 
@@ -52,6 +56,10 @@ std::string print_like_reference(double x);
 // Every unsuffixed floating literal outside comments, strings and character
 // constants gets an `f` suffix (fp32 programs).
 std::string suffix_float_literals(const std::string &src);
+
+// Shared memory words (real_t) of one orbit in the lanes-per-orbit kernel;
+// must match SODECL_SLOT in device/solvers.cuh.
+int lanes_slot_words(const ProgramSpec &spec);
 
 // Assembles the program text.
 std::string assemble(const ProgramSpec &spec, const std::string &system_src, const SystemTraits &traits);
@@ -73,6 +81,10 @@ struct BatchClass {
     ProgramSpec spec;
     std::string system_src;
 };
+
+// Doubles of dynamic shared memory each warp of the batch kernel needs: the
+// largest (32 / lanes) x slot of the classes with lanes per orbit, else 0.
+int batch_warp_words(const std::vector<BatchClass> &classes);
 
 // All classes in one program with the persistent kernel `sodecl_batch`.
 std::shared_ptr<const Program> build_batch(const std::vector<BatchClass> &classes, bool fmad, bool fast_div,

@@ -207,21 +207,74 @@ int ensure_gpu(sodecl_ctx *ctx)
     return SODECL_OK;
 }
 
-int block_size(const sodecl_ctx *ctx)
+int lanes_of(const sodecl_cfg &c) { return c.lanes_per_orbit > 1 ? c.lanes_per_orbit : 1; }
+
+// Whether the system file has the per-row functions lanes per orbit need
+// with this solver.
+bool lanes_supported(const sodecl_b200::SystemTraits &t, int solver)
 {
-    return ctx->cfg.local_group_size > 0 ? ctx->cfg.local_group_size : kDefaultBlock;
+    if (!t.has_row) return false;
+    if (solver == SODECL_STOCHASTIC_EULER) return t.has_stoch_row;
+    if (solver == SODECL_IMPLICIT_EULER || solver == SODECL_IMPLICIT_MIDPOINT) return t.has_jac_band;
+    return true;
+}
+
+// Shared memory cap of one block of the lanes-per-orbit kernel (the default
+// dynamic shared memory limit, no opt-in needed).
+constexpr size_t kLanesSharedCap = 48 * 1024;
+
+// Launch geometry of the configured kernel for n orbits: threads per block,
+// blocks, dynamic shared memory.  One thread per orbit: the block size as
+// configured.  Lanes per orbit: a multiple of 32 threads, reduced until the
+// block's orbit slots fit kLanesSharedCap.
+struct Geometry {
+    int block = 0;
+    long long grid = 0;
+    size_t shared = 0;
+};
+
+Geometry geometry(const sodecl_cfg &c, int64_t n)
+{
+    Geometry g;
+    int block = c.local_group_size > 0 ? c.local_group_size : kDefaultBlock;
+    const int lanes = lanes_of(c);
+    if (lanes == 1) {
+        g.block = block;
+        g.grid = (n + block - 1) / block;
+        return g;
+    }
+    block = std::max(32, (block + 31) / 32 * 32);
+    ProgramSpec spec;
+    spec.solver = c.solver;
+    spec.num_equat = c.num_equat;
+    spec.num_params = c.num_params;
+    spec.num_noi = c.num_noi;
+    const size_t slot = static_cast<size_t>(sodecl_b200::lanes_slot_words(spec)) *
+                        (c.precision == SODECL_FP32 ? sizeof(float) : sizeof(double));
+    while (block > 32 && static_cast<size_t>(block / lanes) * slot > kLanesSharedCap) block -= 32;
+    g.block = block;
+    g.grid = (n * lanes + block - 1) / block;
+    g.shared = static_cast<size_t>(block / lanes) * slot;
+    return g;
+}
+
+int launch_kernel(sodecl_ctx *ctx, cudaKernel_t kernel, const sodecl_cfg &c, const DeviceArgs &a, cudaStream_t stream)
+{
+    if (a.n <= 0) return SODECL_OK;
+    const Geometry g = geometry(c, a.n);
+    if (g.grid > 0x7fffffffLL) return ctx->fail(SODECL_ERR_INVALID_ARG, "too many orbits for one launch");
+    if (g.shared > kLanesSharedCap)
+        return ctx->fail(SODECL_ERR_UNSUPPORTED, "one orbit's state, parameters and noise exceed the shared memory of a "
+                                                 "block: use one thread per orbit");
+    void *args[] = {const_cast<DeviceArgs *>(&a)};
+    SODECL_CUDA_TRY(ctx, cudaLaunchKernel(reinterpret_cast<const void *>(kernel), dim3(static_cast<unsigned>(g.grid)),
+                                          dim3(g.block), args, g.shared, stream));
+    return SODECL_OK;
 }
 
 int launch(sodecl_ctx *ctx, const DeviceArgs &a, cudaStream_t stream)
 {
-    if (a.n <= 0) return SODECL_OK;
-    const int block = block_size(ctx);
-    const long long grid = (a.n + block - 1) / block;
-    if (grid > 0x7fffffffLL) return ctx->fail(SODECL_ERR_INVALID_ARG, "too many orbits for one launch");
-    void *args[] = {const_cast<DeviceArgs *>(&a)};
-    SODECL_CUDA_TRY(ctx, cudaLaunchKernel(reinterpret_cast<const void *>(ctx->kernel), dim3(static_cast<unsigned>(grid)),
-                                          dim3(block), args, 0, stream));
-    return SODECL_OK;
+    return launch_kernel(ctx, ctx->kernel, ctx->cfg, a, stream);
 }
 
 ProgramSpec make_spec(const sodecl_cfg &c)
@@ -239,9 +292,12 @@ ProgramSpec make_spec(const sodecl_cfg &c)
     spec.record_f32 = c.record_f32 != 0;
     spec.newton_tol = c.newton_tol;
     spec.newton_max_iter = c.newton_max_iter;
-    spec.block_max = std::max(256, c.local_group_size > 0 ? c.local_group_size : kDefaultBlock);
+    // lanes per orbit round the block up to whole warps
+    const int block = c.local_group_size > 0 ? c.local_group_size : kDefaultBlock;
+    spec.block_max = std::max(256, c.lanes_per_orbit > 1 ? (block + 31) / 32 * 32 : block);
     spec.min_blocks = c.min_blocks_per_sm;
     spec.fast_div = c.division == SODECL_DIV_RECIPROCAL;
+    spec.lanes = lanes_of(c);
     return spec;
 }
 
@@ -310,6 +366,8 @@ int sodecl_cuda_create(const sodecl_cfg *cfg, sodecl_ctx **out)
     if (c.newton_tol < 0 || !std::isfinite(c.newton_tol) || c.newton_max_iter < 0) return SODECL_ERR_INVALID_ARG;
     if (c.min_blocks_per_sm < 0 || c.min_blocks_per_sm > 32) return SODECL_ERR_INVALID_ARG;
     if (c.division != SODECL_DIV_RECIPROCAL && c.division != SODECL_DIV_IEEE) return SODECL_ERR_INVALID_ARG;
+    if (c.lanes_per_orbit < 0 || c.lanes_per_orbit > 32 || (c.lanes_per_orbit & (c.lanes_per_orbit - 1)) != 0)
+        return SODECL_ERR_INVALID_ARG;
     const int64_t nchunks = count_chunks(c);
     if (nchunks > 0x7ffffffeLL) return SODECL_ERR_INVALID_ARG;
     auto *ctx = new (std::nothrow) sodecl_ctx();
@@ -334,6 +392,14 @@ int sodecl_cuda_compile(sodecl_ctx *ctx, const char *system_src, size_t len)
         return ctx->fail(SODECL_ERR_NO_JACOBIAN, "implicit solvers need calc_jacobian(...) in the system file");
     if (solver == SODECL_STOCHASTIC_EULER && !traits.has_stoch)
         return ctx->fail(SODECL_ERR_NO_STOCH, "the stochastic solver needs sode_system_stoch(...) in the system file");
+    if (lanes_of(ctx->cfg) > 1) {
+        if (!lanes_supported(traits, solver))
+            return ctx->fail(SODECL_ERR_UNSUPPORTED, "lanes per orbit need sode_system_row(...) in the system file, "
+                                                     "and sode_system_stoch_row(...) for the stochastic solver or "
+                                                     "calc_jacobian_band(...) for the implicit ones");
+        if (geometry(ctx->cfg, 1).shared > kLanesSharedCap)
+            return ctx->fail(SODECL_ERR_UNSUPPORTED, "lanes per orbit: one orbit does not fit a block's shared memory");
+    }
     ProgramSpec spec = make_spec(ctx->cfg);
     try {
         auto prog = sodecl_b200::build(spec, src);
@@ -592,7 +658,7 @@ int sodecl_cuda_kernel_info(sodecl_ctx *ctx, int *regs, int *local_bytes, int *m
 }
 
 int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_steps, int32_t *block,
-                         int32_t *min_blocks, int32_t *division, double *best_ms)
+                         int32_t *min_blocks, int32_t *division, int32_t *lanes, double *best_ms)
 {
     if (!ctx) return SODECL_ERR_INVALID_ARG;
     if (!ctx->uploaded) return ctx->fail(SODECL_ERR_STATE, "upload the orbits first: the tuner samples them");
@@ -615,19 +681,30 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
     (void)npar;
 
     struct Cand {
-        int block, min_blocks, division;
+        int block, min_blocks, division, lanes;
     };
-    std::vector<Cand> cands = {{128, 0, SODECL_DIV_IEEE}, {128, 4, SODECL_DIV_IEEE}, {256, 3, SODECL_DIV_IEEE},
-                               {64, 0, SODECL_DIV_IEEE}};
+    std::vector<Cand> cands = {{128, 0, SODECL_DIV_IEEE, 1}, {128, 4, SODECL_DIV_IEEE, 1},
+                               {256, 3, SODECL_DIV_IEEE, 1}, {64, 0, SODECL_DIV_IEEE, 1}};
     if (ctx->cfg.precision == SODECL_FP64) {
-        cands.push_back({128, 0, SODECL_DIV_RECIPROCAL});
-        cands.push_back({128, 4, SODECL_DIV_RECIPROCAL});
+        cands.push_back({128, 0, SODECL_DIV_RECIPROCAL, 1});
+        cands.push_back({128, 4, SODECL_DIV_RECIPROCAL, 1});
+    }
+    // lanes per orbit: up to the first power of two >= the equations
+    const auto traits = sodecl_b200::inspect_system(ctx->system_src);
+    const int solver = ctx->cfg.solver;
+    const bool row_ok = lanes_supported(traits, solver);
+    if (row_ok) {
+        for (int l = 2; l <= 32 && l / 2 < ctx->cfg.num_equat; l *= 2) {
+            if (l < 4) continue;
+            cands.push_back({128, 0, SODECL_DIV_IEEE, l});
+            cands.push_back({256, 0, SODECL_DIV_IEEE, l});
+        }
     }
     const sodecl_cfg saved = ctx->cfg;
     auto saved_prog = ctx->prog;
     double best = 1e300;
     Cand pick = {saved.local_group_size > 0 ? saved.local_group_size : kDefaultBlock, saved.min_blocks_per_sm,
-                 saved.division};
+                 saved.division, lanes_of(saved)};
     cudaEvent_t e0, e1;
     SODECL_CUDA_TRY(ctx, cudaEventCreate(&e0));
     SODECL_CUDA_TRY(ctx, cudaEventCreate(&e1));
@@ -637,6 +714,8 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
         cfg.local_group_size = c.block;
         cfg.min_blocks_per_sm = c.min_blocks;
         cfg.division = c.division;
+        cfg.lanes_per_orbit = c.lanes;
+        if (c.lanes > 1 && geometry(cfg, 1).shared > kLanesSharedCap) continue;
         std::shared_ptr<const Program> prog;
         try {
             prog = sodecl_b200::build(make_spec(cfg), ctx->system_src);
@@ -666,14 +745,13 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
             a.rec_stride = n;
             a.chunk_begin = 0;
             a.chunk_end = chunks;
-            void *args[] = {&a};
             cudaEventRecord(e0, ctx->stream);
-            cudaError_t le = cudaLaunchKernel(reinterpret_cast<const void *>(kern),
-                                              dim3(static_cast<unsigned>((n + c.block - 1) / c.block)), dim3(c.block),
-                                              args, 0, ctx->stream);
+            rc = launch_kernel(ctx, kern, cfg, a, ctx->stream);
             cudaEventRecord(e1, ctx->stream);
-            if (le != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
-                rc = cuda_fail(ctx, le != cudaSuccess ? le : cudaErrorUnknown, "autotune launch");
+            if (rc != SODECL_OK) break;
+            const cudaError_t se = cudaEventSynchronize(e1);
+            if (se != cudaSuccess) {
+                rc = cuda_fail(ctx, se, "autotune launch");
                 break;
             }
             cudaEventElapsedTime(&ms, e0, e1);
@@ -692,6 +770,7 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
     ctx->cfg.local_group_size = pick.block;
     ctx->cfg.min_blocks_per_sm = pick.min_blocks;
     ctx->cfg.division = pick.division;
+    ctx->cfg.lanes_per_orbit = pick.lanes;
     try {
         auto prog = sodecl_b200::build(make_spec(ctx->cfg), ctx->system_src);
         if (prog != ctx->prog) {
@@ -710,6 +789,7 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
     if (block) *block = pick.block;
     if (min_blocks) *min_blocks = pick.min_blocks;
     if (division) *division = pick.division;
+    if (lanes) *lanes = pick.lanes;
     if (best_ms) *best_ms = best;
     return SODECL_OK;
 }

@@ -101,14 +101,19 @@ def trajectory_mse(params, y0, t0, targets, adjoint):
 def finite_difference_gradient(t0, y0, params, targets, adjoint_wide, rel_step=1e-6):
     """Central differences of the per-orbit loss w.r.t. every parameter and
     initial value, all 2 x (npar + neq) perturbed copies of every orbit in one
-    launch of the loss kernel.  `adjoint_wide` must wrap an integrator sized
-    for n * 2 * (npar + neq) orbits.  Returns (grad_params, grad_y0)."""
+    launch of the loss kernel.  The step of each entry is rel_step x its
+    magnitude (rel_step itself for entries that are exactly zero): an absolute
+    floor would be far too coarse for small parameters such as the
+    oculomotor model's 0.0045 time constant, whose loss curves as 1/p.
+    `adjoint_wide` must wrap an integrator sized for n * 2 * (npar + neq)
+    orbits.  Returns (grad_params, grad_y0)."""
     torch = _torch()
     n, npar = params.shape
     neq = y0.shape[1]
     k = npar + neq
     theta = torch.cat([params, y0], dim=1)                              # [n, k]
-    h = rel_step * torch.clamp(theta.abs(), min=1.0)                    # [n, k]
+    mag = theta.abs()
+    h = rel_step * torch.where(mag > 0, mag, torch.ones_like(mag))       # [n, k]
     eye = torch.eye(k, dtype=theta.dtype, device=theta.device)
     sign = torch.tensor([1.0, -1.0], dtype=theta.dtype, device=theta.device)
     # pert[s, d, i] = theta[i] + sign[s] * h[i, d] * e_d, copies ordered [sign][direction][orbit]
@@ -119,5 +124,7 @@ def finite_difference_gradient(t0, y0, params, targets, adjoint_wide, rel_step=1
     loss, _, _, _ = adjoint_wide(rep(t0), pert[:, npar:].contiguous(), pert[:, :npar].contiguous(), tgt,
                                  with_gradient=False)
     loss = loss.reshape(2, k, n)
-    g = (loss[0] - loss[1]) / (2.0 * h.T)                               # [k, n]
+    # divide by the perturbation the rounded copies actually carry
+    up, down = theta.T + h.T, theta.T - h.T                             # [k, n]
+    g = (loss[0] - loss[1]) / (up - down)                               # [k, n]
     return g[:npar].T.contiguous(), g[npar:].T.contiguous()

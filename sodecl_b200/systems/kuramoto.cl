@@ -13,6 +13,11 @@
  * this library's addition so the implicit solvers can integrate it:
  *   J_ij = (K/N) cos(theta_j - theta_i)               (j != i)
  *   J_ii = -(K/N) sum_{j != i} cos(theta_j - theta_i)
+ * `sode_system_row`, `sode_system_stoch_row` and `calc_jacobian_band` (also
+ * additions) give one equation's terms and its row's three band entries
+ * (columns i-1, i, i+1), evaluated exactly as `sode_system`,
+ * `sode_system_stoch` and `calc_jacobian` evaluate them; with them, several
+ * lanes of a warp can share one orbit (lanes per orbit).
  */
 
 void sode_system(double t, double y[_numeq_], double yout[_numeq_], double p[_numpar_])
@@ -27,6 +32,17 @@ void sode_system(double t, double y[_numeq_], double yout[_numeq_], double p[_nu
 		coupling = coupling * (double)(p[0] / (double)(_numeq_));
 		yout[i] = coupling + p[i + 1];
 	}
+}
+
+double sode_system_row(int i, double t, double y[_numeq_], double p[_numpar_])
+{
+	double coupling = 0;
+	for (int j = 0; j < _numeq_; j++)
+	{
+		coupling = coupling + (sin(y[j] - y[i]));
+	}
+	coupling = coupling * (double)(p[0] / (double)(_numeq_));
+	return coupling + p[i + 1];
 }
 
 void calc_jacobian(double y[_numeq_], double jac[_numeq_][_numeq_], double p[_numpar_])
@@ -48,10 +64,40 @@ void calc_jacobian(double y[_numeq_], double jac[_numeq_][_numeq_], double p[_nu
 	}
 }
 
+void calc_jacobian_band(int i, double y[_numeq_], double band[3], double p[_numpar_])
+{
+	double scale = (double)(p[0] / (double)(_numeq_));
+	double diag = 0;
+	band[0] = 0;
+	band[2] = 0;
+	for (int j = 0; j < _numeq_; j++)
+	{
+		double c = scale * cos(y[j] - y[i]);
+		if (j == i - 1)
+		{
+			band[0] = c;
+		}
+		if (j == i + 1)
+		{
+			band[2] = c;
+		}
+		if (j != i)
+		{
+			diag = diag - c;
+		}
+	}
+	band[1] = diag;
+}
+
 void sode_system_stoch(double t, double y[_numeq_], double stoch[_numeq_], double p[_numpar_], double noise[_numnoi_])
 {
 	for (int i = 0; i < _numeq_; i++)
 	{
 		stoch[i] = p[_numpar_ - _numnoi_ + i] * noise[i];
 	}
+}
+
+double sode_system_stoch_row(int i, double t, double y[_numeq_], double p[_numpar_], double noise[_numnoi_])
+{
+	return p[_numpar_ - _numnoi_ + i] * noise[i];
 }

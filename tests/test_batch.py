@@ -152,3 +152,47 @@ def test_batch_tuner_and_launch_shapes_agree():
     b.set_items(cls, nsteps, t0, y0, p, counters)
     block, bps, ms = b.tune()
     assert block in (64, 128, 256) and ms > 0
+
+
+# (system, solver, neq, npar, nnoi, dt, lanes): wide classes with lanes per orbit
+# (0: automatic), next to one-lane classes in the same program
+LANES_CLASSES = [("kuramoto", "ie", 64, 65, 0, 0.01, 32), ("kuramoto", "se", 32, 65, 32, 0.01, 0),
+                 ("kuramoto", "rk4", 16, 17, 0, 0.01, 4), ("kuramoto", "euler", 12, 13, 0, 0.01, 0),
+                 ("kuramoto", "im", 20, 21, 0, 0.01, 8), ("kuramoto", "rk4", 4, 5, 0, 0.01, 0),
+                 ("oculomotor", "ie", 6, 6, 0, 1e-3, 0)]
+
+
+def test_batch_lanes_program_builds_without_gpu():
+    b = Batch(fmad=False)
+    for system, solver, neq, npar, nnoi, dt, lanes in LANES_CLASSES:
+        b.add_class(system_path(system), solver, neq=neq, npar=npar, nnoi=nnoi, dt=dt, lanes=lanes)
+    text = b.compile().program_source
+    lanes = [int(x) for x in re.findall(r"#define SODECL_NEWTON_MAX \d+\n#define SODECL_LANES (\d+)", text)]
+    assert lanes == [32, 16, 4, 8, 8, 1, 1]
+    assert re.search(r"#define SODECL_BATCH_WARP_WORDS [1-9]\d*", text)
+    with pytest.raises(N.SodeclError) as e:
+        Batch().add_class(system_path("oculomotor"), "rk4", neq=6, npar=6, dt=1e-5, lanes=4)
+    assert e.value.status == N.ERR_UNSUPPORTED
+
+
+@pytest.mark.gpu
+def test_batch_lanes_classes_match_single_system_kernel_bit_for_bit():
+    classes = [c[:6] for c in LANES_CLASSES]
+    b = Batch(fmad=False)
+    for system, solver, neq, npar, nnoi, dt, lanes in LANES_CLASSES:
+        b.add_class(system_path(system), solver, neq=neq, npar=npar, nnoi=nnoi, dt=dt, lanes=lanes)
+    b.compile()
+    n = 700
+    cls, nsteps, t0, y0, p, counters = make_items(n, 5, classes=classes, steps=(0, 1, 7, 50, 123))
+    b.set_items(cls, nsteps, t0, y0, p, counters)
+    b.run(graph=True)
+    t, y, cnt, passes, flags = b.results()
+    rng = np.random.default_rng(6)
+    for i in rng.choice(n, 50, replace=False):
+        system, solver, neq, npar, nnoi, dt = classes[cls[i]]
+        tt, yy, cc = single_kernel_final_state(system, solver, neq, npar, nnoi, dt, nsteps[i], t0[i], y0[i], p[i],
+                                               counters[i], i, False)
+        np.testing.assert_array_equal(y[i], yy)
+        assert t[i] == tt
+        if nnoi:
+            assert cnt[i] == cc
