@@ -300,7 +300,7 @@ struct sodecl_adjoint_args {
 };
 
 // Loss and, if grad_p is set, its gradient for every orbit.
-extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX) sodecl_adjoint(const sodecl_adjoint_args a)
+extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS) sodecl_adjoint(const sodecl_adjoint_args a)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;

@@ -544,17 +544,20 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
     return s.str();
 }
 
-std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, int tape_cap, bool analytic)
+std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, int tape_cap, bool analytic,
+                             bool fast_div)
 {
     const SystemTraits tr = inspect_system(src);
     std::ostringstream s;
     s << "// SODECL adjoint program generated by libsodecl_cuda (sm_100a)\n";
-    s << "#define SODECL_STEPS_ONLY 1\n#define SODECL_FP32 0\n#define SODECL_RECORD_F32 0\n#define SODECL_FAST_DIV 0\n";
+    s << "#define SODECL_STEPS_ONLY 1\n#define SODECL_FP32 0\n#define SODECL_RECORD_F32 0\n";
+    s << "#define SODECL_FAST_DIV " << (fast_div ? 1 : 0) << "\n";
     s << "#define SODECL_SOLVER " << spec.solver << "\n";
     s << "#define SODECL_HAS_JACOBIAN " << (tr.has_jacobian ? 1 : 0) << "\n";
     s << "#define SODECL_HAS_STOCH " << (tr.has_stoch ? 1 : 0) << "\n";
     s << "#define SODECL_NEWTON_MAX " << spec.newton_max_iter << "\n";
     s << "#define SODECL_BLOCK_MAX " << spec.block_max << "\n";
+    if (spec.min_blocks > 0) s << "#define SODECL_MIN_BLOCKS " << spec.min_blocks << "\n";
     s << "#define SODECL_TAPE_CAP " << tape_cap << "\n";
     s << "#define SODECL_ADJ_ANALYTIC " << (analytic ? 1 : 0) << "\n";
     s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n" << kAdjointSrc << "\n";
@@ -567,7 +570,9 @@ std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, in
     s << "#define _epsilon1_ " << print_like_reference(spec.newton_tol) << "\n";
     const std::string user = relax_parameter_bounds(src);
     const std::vector<std::string> macros = defined_macros(src);
+    if (fast_div) s << "#define double sodecl_f64\n";
     s << "#line 1 \"system.cl\"\n" << user << "\n";
+    if (fast_div) s << "#undef double\n";
     for (const auto &m : macros) s << "#undef " << m << "\n";
     // the recording copy: every double of the system file is a sodecl_ad
     s << "namespace sodecl_adsys {\n#define double sodecl_ad\n#line 1 \"system.cl\"\n" << user
@@ -583,7 +588,16 @@ std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, in
 std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std::string &system_src, int tape_cap,
                                              bool analytic)
 {
-    return compile_text(assemble_adjoint(spec, system_src, tape_cap, analytic), spec.fmad, false, "sodecl_adjoint");
+    // the reciprocal quotients only where the system file is plain arithmetic
+    if (spec.fast_div && system_src.find("printf") == std::string::npos) {
+        try {
+            return compile_text(assemble_adjoint(spec, system_src, tape_cap, analytic, true), spec.fmad, true,
+                                "sodecl_adjoint");
+        } catch (const std::exception &) {
+        }
+    }
+    return compile_text(assemble_adjoint(spec, system_src, tape_cap, analytic, false), spec.fmad, false,
+                        "sodecl_adjoint");
 }
 
 std::shared_ptr<const Program> build_batch(const std::vector<BatchClass> &classes, bool fmad, bool fast_div,

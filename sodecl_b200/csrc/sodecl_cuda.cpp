@@ -98,6 +98,7 @@ struct sodecl_ctx {
 
     // discrete adjoint: its own program and scratch (checkpoints, segments)
     std::shared_ptr<const Program> adj_prog;
+    int adj_min_blocks = -1;
     cudaLibrary_t adj_lib = nullptr;
     cudaKernel_t adj_kernel = nullptr;
     int adj_tape = 0;
@@ -816,9 +817,23 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     const int tape = io->tape_entries > 0 ? io->tape_entries : 256;
     const auto traits = sodecl_b200::inspect_system(ctx->system_src);
     const bool analytic = !io->use_tape && traits.has_jacobian && traits.has_pjacobian;
-    if (!ctx->adj_prog || ctx->adj_tape != tape || ctx->adj_analytic != analytic) {
+    // Resident blocks the compiler must allow for (a register cap): enough
+    // that every orbit gets a thread in the first wave, up to 4 blocks of 128
+    // (128 registers).  Each thread runs its orbit's whole forward and
+    // backward sweep, so a second wave would double the time.
+    int sms = 148;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device) != cudaSuccess) {
+        cudaGetLastError();
+        sms = 148;
+    }
+    const long long per_wave = static_cast<long long>(std::max(1, sms)) * 128;
+    const long long waves = (io->n + per_wave - 1) / per_wave;
+    const int min_blocks = waves <= 2 ? 0 : static_cast<int>(std::min<long long>(4, waves));
+    if (!ctx->adj_prog || ctx->adj_tape != tape || ctx->adj_analytic != analytic || ctx->adj_min_blocks != min_blocks) {
         try {
             ProgramSpec spec = make_spec(ctx->cfg);
+            spec.block_max = 128;
+            spec.min_blocks = min_blocks;
             auto prog = sodecl_b200::build_adjoint(spec, ctx->system_src, tape, analytic);
             if (ctx->adj_lib) cudaLibraryUnload(ctx->adj_lib);
             ctx->adj_lib = nullptr;
@@ -826,6 +841,7 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
             ctx->adj_prog = prog;
             ctx->adj_tape = tape;
             ctx->adj_analytic = analytic;
+            ctx->adj_min_blocks = min_blocks;
         } catch (const std::exception &ex) {
             return ctx->fail(SODECL_ERR_COMPILE, ex.what());
         }

@@ -16,8 +16,9 @@
  * Same model and the same floating-point evaluation order as the
  * reference's examples/oculomotor.cl (sburstf :5-20, dsburstf :22-36,
  * calc_jacobian :38-81, sode_system :83-97, sode_system_stoch :99-112),
- * so trajectories agree with the reference to the last bits.  Two
- * differences, neither of which changes a trajectory: jac[4][5] carries the
+ * so trajectories agree with the reference to the last bits.  Three
+ * differences, none of which changes a trajectory: ocm_burst selects its exp
+ * argument instead of branching (same values, see there); jac[4][5] carries the
  * chain-rule sign the reference's calc_jacobian omits (entries off the three
  * bands are never read by the implicit solvers), and calc_jacobian_params
  * (df/dp, for the adjoint) is an addition.
@@ -30,19 +31,18 @@
 #define OCM_VEL_GAIN ((1.00 / OCM_T1) + (1.00 / OCM_T2))
 #define OCM_POS_GAIN (1.00 / (OCM_T1 * OCM_T2))
 
-/* burst-neuron firing-rate non-linearity */
+/* burst-neuron firing-rate non-linearity:
+ *   x > 0:  at * (1 - exp(-x / bt))
+ *   else:   -(a / b) * x * exp(x / b)
+ * written with one exp whose argument is selected: x / (-bt) rounds exactly
+ * as (-x) / bt, so each branch's value is the same to the last bit, and the
+ * orbits of a warp on either side of x = 0 share one exp instead of running
+ * both branches one after the other */
 double ocm_burst(double x, double a, double b, double at, double bt)
 {
-	double rate = 0;
-	if (x > 0)
-	{
-		rate = (at * (1.00 - exp(-x / bt)));
-	}
-	else
-	{
-		rate = (-(a / b) * x * exp(x / b));
-	}
-	return rate;
+	int right = x > 0;
+	double e = exp(x / (right ? -bt : b));
+	return right ? (at * (1.00 - e)) : (-(a / b) * x * e);
 }
 
 /* d(ocm_burst)/dx */
@@ -108,30 +108,26 @@ void calc_jacobian(double y[_numeq_], double jac[_numeq_][_numeq_], double p[_nu
 	jac[5][4] = 1;
 }
 
-/* d(ocm_burst)/d(a, b, at, bt) */
-void ocm_burst_dparams(double x, double a, double b, double at, double bt, double d[4])
+/* ocm_burst(x, ...) and its derivatives d[0..3] w.r.t. (a, b, at, bt), with
+ * one exp (argument selected as in ocm_burst) */
+double ocm_burst_dparams(double x, double a, double b, double at, double bt, double d[4])
 {
-	if (x > 0)
-	{
-		double e = exp(-x / bt);
-		d[0] = 0;
-		d[1] = 0;
-		d[2] = 1.00 - e;
-		d[3] = -(at * x * e) / (bt * bt);
-	}
-	else
-	{
-		double e = exp(x / b);
-		d[0] = -(x * e) / b;
-		d[1] = (a * x * e) / (b * b) * (1.00 + x / b);
-		d[2] = 0;
-		d[3] = 0;
-	}
+	int right = x > 0;
+	double e = exp(x / (right ? -bt : b));
+	double ib = 1.00 / b;
+	double ibt = 1.00 / bt;
+	d[0] = right ? (double)0 : -(x * e) * ib;
+	d[1] = right ? (double)0 : (a * x * e) * ib * ib * (1.00 + x * ib);
+	d[2] = right ? 1.00 - e : (double)0;
+	d[3] = right ? -(at * x * e) * ibt * ibt : (double)0;
+	return right ? (at * (1.00 - e)) : (-(a * ib) * x * e);
 }
 
 /* df/dp, jacp[i][k] = d yout[i] / d p[k] for the six model parameters.  Not in
  * the reference's file: the adjoint (model fitting) uses it together with
- * calc_jacobian; without it the adjoint differentiates sode_system itself. */
+ * calc_jacobian; without it the adjoint differentiates sode_system itself.
+ * Only gradients depend on it, so it shares subexpressions freely (one exp per
+ * burst, one reciprocal of tau). */
 void calc_jacobian_params(double y[_numeq_], double jacp[_numeq_][_numpar_], double p[_numpar_])
 {
 	int i, k;
@@ -143,22 +139,23 @@ void calc_jacobian_params(double y[_numeq_], double jacp[_numeq_][_numpar_], dou
 			jacp[i][k] = 0;
 		}
 	}
-	ocm_burst_dparams(y[5], p[0], p[1], p[4], p[5], dr);
-	ocm_burst_dparams(-y[5], p[0], p[1], p[4], p[5], dl);
-	double r = -y[3] - (p[3] * y[3] * y[4] * y[4]) + ocm_burst(y[5], p[0], p[1], p[4], p[5]);
-	double l = -y[4] - (p[3] * y[4] * y[3] * y[3]) + ocm_burst(-y[5], p[0], p[1], p[4], p[5]);
-	jacp[3][0] = dr[0] / p[2];
-	jacp[3][1] = dr[1] / p[2];
-	jacp[3][2] = -r / (p[2] * p[2]);
-	jacp[3][3] = -(y[3] * y[4] * y[4]) / p[2];
-	jacp[3][4] = dr[2] / p[2];
-	jacp[3][5] = dr[3] / p[2];
-	jacp[4][0] = dl[0] / p[2];
-	jacp[4][1] = dl[1] / p[2];
-	jacp[4][2] = -l / (p[2] * p[2]);
-	jacp[4][3] = -(y[4] * y[3] * y[3]) / p[2];
-	jacp[4][4] = dl[2] / p[2];
-	jacp[4][5] = dl[3] / p[2];
+	double itau = 1.00 / p[2];
+	double br = ocm_burst_dparams(y[5], p[0], p[1], p[4], p[5], dr);
+	double bl = ocm_burst_dparams(-y[5], p[0], p[1], p[4], p[5], dl);
+	double r = -y[3] - (p[3] * y[3] * y[4] * y[4]) + br;
+	double l = -y[4] - (p[3] * y[4] * y[3] * y[3]) + bl;
+	jacp[3][0] = dr[0] * itau;
+	jacp[3][1] = dr[1] * itau;
+	jacp[3][2] = -r * itau * itau;
+	jacp[3][3] = -(y[3] * y[4] * y[4]) * itau;
+	jacp[3][4] = dr[2] * itau;
+	jacp[3][5] = dr[3] * itau;
+	jacp[4][0] = dl[0] * itau;
+	jacp[4][1] = dl[1] * itau;
+	jacp[4][2] = -l * itau * itau;
+	jacp[4][3] = -(y[4] * y[3] * y[3]) * itau;
+	jacp[4][4] = dl[2] * itau;
+	jacp[4][5] = dl[3] * itau;
 }
 
 void sode_system_stoch(double t, double y[_numeq_], double stoch[_numeq_], double p[_numpar_], double noise[_numnoi_])

@@ -1,0 +1,160 @@
+"""Seeded synthetic workloads of the benchmark shapes, and a command line that
+runs a few launches of one of them (for profiler captures).
+
+    python -m sodecl_b200.workloads stochastic-kuramoto --orbits 32768 --nsteps 200 --lanes 16 --block 256
+
+Shapes (all inputs seeded; no dataset is involved):
+  oculomotor-<solver>   the oculomotor model: parameters uniform within +-50 % of
+                        the nominal (120, 1.5, 0.0045, 0.05, 600, 9), y0 =
+                        (0, 0, 0, 0, 0, 2); default RK4, dt 1e-3, a record every 100
+  stochastic-kuramoto   Kuramoto by Euler-Maruyama: N phases, K ~ U(0,5),
+                        omega ~ N(0,1) shared, additive noise sigma ~ U(0,0.5) per
+                        orbit, counters orbit * 2^20; dt 0.01, a record every 200
+  kuramoto-<solver>     deterministic Kuramoto: N phases, K ~ U(0,5), omega ~ N(0,1)
+                        shared, theta0 ~ U(0, 2 pi); dt 0.01
+  adjoint-oculomotor    loss and gradient (sodecl_cuda_adjoint) of the oculomotor
+                        RK4 fit: targets from seeded true parameters + N(0, 1e-2)
+                        noise, gradient at parameters within +-5 % of them; dt 1e-5
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+
+NOMINAL = np.array([120.0, 1.5, 0.0045, 0.05, 600.0, 9.0])
+Y0 = np.array([0.0, 0.0, 0.0, 0.0, 0.0, 2.0])
+
+
+def oculomotor(n, orbit_offset=0, seed=2024):
+    """(t0, y0, params) of orbits [orbit_offset, orbit_offset + n)."""
+    rng = np.random.default_rng([seed, orbit_offset])
+    params = NOMINAL * rng.uniform(0.5, 1.5, (n, 6))
+    return np.zeros(n), np.tile(Y0, (n, 1)), params
+
+
+def kuramoto(n, N, seed=3, noise=False):
+    """(t0, theta0, params, counters): params = [K, omega_1..N] (+ sigma_1..N,
+    one sigma per orbit, with noise); counters orbit * 2^20 with noise, else None."""
+    rng = np.random.default_rng(seed)
+    cols = [rng.uniform(0, 5, (n, 1)), np.tile(rng.normal(size=N), (n, 1))]
+    if noise:
+        cols.append(np.repeat(rng.uniform(0, 0.5, (n, 1)), N, axis=1))
+    params = np.concatenate(cols, axis=1)
+    theta0 = rng.uniform(0, 2 * np.pi, (n, N))
+    counters = np.arange(n) * 2.0 ** 20 if noise else None
+    return np.zeros(n), theta0, params, counters
+
+
+def fitting_targets(n, nsteps, ksteps, dt, seed=55, device="cuda"):
+    """(t0, y0, guess params, targets[records, 6, n]) of the oculomotor fit."""
+    import torch
+
+    from . import Integrator, system_path
+
+    rng = np.random.default_rng(seed)
+    true_p = NOMINAL * rng.uniform(0.5, 1.5, (n, 6))
+    guess = true_p * rng.uniform(0.95, 1.05, (n, 6))
+    y0 = np.tile(Y0, (n, 1))
+    sim = Integrator(system_path("oculomotor"), "rk4", dt=dt, tspan=(nsteps - 0.5) * dt, ksteps=ksteps, neq=6,
+                     npar=6, orbits=n)
+    T = lambda x: torch.tensor(x, device=device)  # noqa: E731
+    rec = torch.empty((sim.num_records, 6, n), dtype=torch.float64, device=device)
+    td, yd, pd = T(np.zeros(n)), T(y0), T(true_p)
+    sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(), records=rec.data_ptr(),
+               stream=torch.cuda.current_stream(device).cuda_stream)
+    gen = torch.Generator(device=device).manual_seed(7)
+    targets = rec + 1e-2 * torch.randn(rec.shape, dtype=torch.float64, device=device, generator=gen)
+    torch.cuda.synchronize()
+    sim.close()
+    return np.zeros(n), y0, guess, targets
+
+
+def _adjoint_main(a):
+    import torch
+
+    from . import Integrator, system_path
+    from .fit import Adjoint
+
+    dt = a.dt if a.dt is not None else 1e-5
+    t0, y0, guess, targets = fitting_targets(a.orbits, a.nsteps, a.ksteps, dt)
+    sim = Integrator(system_path("oculomotor"), "rk4", dt=dt, tspan=(a.nsteps - 0.5) * dt, ksteps=a.ksteps, neq=6,
+                     npar=6, orbits=a.orbits)
+    T = lambda x: torch.tensor(x, device="cuda")  # noqa: E731
+    adj = Adjoint(sim)
+    for k in range(a.launches):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        adj(T(t0), T(y0), T(guess), targets)
+        e.record()
+        torch.cuda.synchronize()
+        print(json.dumps({"case": a.case, "launch": k, "ms": s.elapsed_time(e), "orbits": a.orbits,
+                          "nsteps": a.nsteps}), flush=True)
+
+
+def _parse():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("case", help="oculomotor-<solver> | stochastic-kuramoto | kuramoto-<solver>")
+    ap.add_argument("--orbits", type=int, default=1 << 15)
+    ap.add_argument("--nsteps", type=int, default=200)
+    ap.add_argument("--ksteps", type=int, default=100)
+    ap.add_argument("--dt", type=float, default=None)
+    ap.add_argument("--N", type=int, default=32, help="Kuramoto phases")
+    ap.add_argument("--lanes", type=int, default=1)
+    ap.add_argument("--block", type=int, default=0)
+    ap.add_argument("--precision", default="fp64")
+    ap.add_argument("--launches", type=int, default=2)
+    return ap.parse_args()
+
+
+def main():
+    import torch
+
+    from . import Integrator, system_path
+
+    a = _parse()
+    n = a.orbits
+    if a.case == "adjoint-oculomotor":
+        return _adjoint_main(a)
+    if a.case.startswith("oculomotor"):
+        solver = a.case.split("-", 1)[1] if "-" in a.case else "rk4"
+        dt = a.dt if a.dt is not None else 1e-3
+        t0, y0, p = oculomotor(n)
+        cnt, system, neq, nnoi = None, "oculomotor", 6, 0
+    elif a.case == "stochastic-kuramoto":
+        solver, dt = "se", a.dt if a.dt is not None else 0.01
+        t0, y0, p, cnt = kuramoto(n, a.N, noise=True)
+        system, neq, nnoi = "kuramoto", a.N, a.N
+    elif a.case.startswith("kuramoto-"):
+        solver, dt = a.case.split("-", 1)[1], a.dt if a.dt is not None else 0.01
+        t0, y0, p, cnt = kuramoto(n, a.N)
+        system, neq, nnoi = "kuramoto", a.N, 0
+    else:
+        raise SystemExit("unknown case " + a.case)
+    sim = Integrator(system_path(system), solver, dt=dt, tspan=a.nsteps * dt, ksteps=a.ksteps, neq=neq,
+                     npar=p.shape[1], nnoi=nnoi, orbits=n, precision=a.precision, lanes=a.lanes, block=a.block)
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    T = lambda x: torch.tensor(x, device=dev)  # noqa: E731
+    td, yd, pd = T(t0), T(y0), T(p)
+    cd = T(cnt) if cnt is not None else None
+    rec = torch.empty((sim.num_records, neq, n), dtype=torch.float64, device=dev)
+    for k in range(a.launches):
+        td.copy_(T(t0))
+        yd.copy_(T(y0))
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(),
+                   counters=cd.data_ptr() if cd is not None else None, records=rec.data_ptr(),
+                   stream=stream.cuda_stream)
+        e.record(stream)
+        torch.cuda.synchronize()
+        ms = s.elapsed_time(e)
+        print(json.dumps({"case": a.case, "launch": k, "ms": ms, "orbit_steps_per_s": n * a.nsteps / (ms * 1e-3),
+                          "lanes": a.lanes, "block": a.block or 128, "orbits": n, "nsteps": a.nsteps}), flush=True)
+    sim.close()
+
+
+if __name__ == "__main__":
+    main()

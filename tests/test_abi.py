@@ -109,7 +109,7 @@ def test_fp32_program_rewrites_literals():
     text = N.program_source(ctx)
     assert "#define double float" in text
     assert "#define OCM_T1 0.15f" in text and "(1.00f / p[2])" in text
-    assert "/* burst-neuron firing-rate non-linearity */" in text  # comments untouched
+    assert "/* burst-neuron firing-rate non-linearity:" in text  # comments untouched
     N.lib.sodecl_cuda_destroy(ctx)
 
 

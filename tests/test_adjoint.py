@@ -167,3 +167,22 @@ def test_system_jacobians_match_central_differences(tmp_path, system, neq, npar,
     print("%s: max rel diff J %.2e, Jp %.2e" % (system, errs[:, 0].max(), errs[:, 1].max()))
     assert errs[:, 0].max() < 1e-5
     assert errs[:, 1].max() < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("use_tape", [False, True])
+def test_adjoint_division_modes_bit_identical(use_tape):
+    """The reciprocal quotient gives IEEE-rounded results, so the adjoint built
+    with it returns the same bits."""
+    torch = pytest.importorskip("torch")
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.fit import Adjoint
+
+    n, nchunks, ksteps, dt = 200, 6, 20, 1e-5
+    t0, y0, p, tg = fitting_problem(n, 4, dt=dt, nchunks=nchunks, ksteps=ksteps)
+    kw = dict(dt=dt, tspan=(nchunks * ksteps - 0.5) * dt, ksteps=ksteps, neq=6, npar=6, orbits=n)
+    T = lambda a: torch.tensor(a, device="cuda")  # noqa: E731
+    out = [Adjoint(Integrator(system_path("oculomotor"), "rk4", division=d, **kw), use_tape=use_tape)(
+        T(t0), T(y0), T(p), T(tg)) for d in ("ieee", "reciprocal")]
+    for a, b in zip(out[0][:3], out[1][:3]):
+        assert torch.equal(a, b)
