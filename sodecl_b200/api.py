@@ -49,7 +49,7 @@ class Integrator:
 
     def __init__(self, system, solver, *, dt, tspan, ksteps, neq, npar, orbits, nnoi=0, device=0,
                  precision="fp64", fmad=True, newton_tol=1e-7, newton_max_iter=1000, block=0,
-                 record_f32=False, min_blocks=0, division="ieee", lanes=1, system_src=None):
+                 record_f32=False, min_blocks=0, division="reciprocal", lanes=1, system_src=None):
         cfg = N.Cfg()
         N.lib.sodecl_cfg_init(C.byref(cfg))
         cfg.solver = _solver_id(solver)

@@ -29,7 +29,7 @@ def _err(b):
 
 
 class Batch:
-    def __init__(self, device=0, fmad=True, division="ieee"):
+    def __init__(self, device=0, fmad=True, division="reciprocal"):
         self._b = C.c_void_p()
         div = N.DIV_RECIPROCAL if division == "reciprocal" else N.DIV_IEEE
         N.check(N.lib.sodecl_batch_create(int(device), 1 if fmad else 0, div, C.byref(self._b)))

@@ -11,11 +11,12 @@
 // within half an ulp of 1/b, q within one ulp of a/b, and the FMA residual
 // is exact as long as nothing under- or overflows -- guaranteed here by
 // requiring |a| and |b| in [2^-500, 2^500); anything else takes the IEEE
-// division.  The point: r = 1/b is a plain division of loop-invariant
-// operands whenever the divisor is a parameter or a constant, so the
+// division, except NaN operands, which return NaN at once.  The point:
+// r = 1/b is a plain division of loop-invariant operands whenever the
+// divisor is a parameter or a constant, so the
 // compiler hoists it out of the step loop and each quotient costs one
 // multiply and two FMAs instead of a full division.  Results are bit-for-bit
-// those of IEEE division.
+// those of IEEE division (a NaN's payload aside).
 __device__ __forceinline__ double sodecl_div_rcp(double a, double b)
 {
     const double r = 1.0 / b;
@@ -26,6 +27,10 @@ __device__ __forceinline__ double sodecl_div_rcp(double a, double b)
     const unsigned eb = ((unsigned)__double2hiint(b) >> 20) & 0x7ffu;
     if ((ea - 523u) < 1000u && (eb - 523u) < 1000u)
         return q2;
+    // a NaN operand makes the quotient NaN (IEEE 754); spare it the division's
+    // special-case path, which orbits that have diverged would take every step
+    if (a != a || b != b)
+        return a + b;
     return a / b;
 }
 

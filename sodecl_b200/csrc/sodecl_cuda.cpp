@@ -103,6 +103,7 @@ struct sodecl_ctx {
     cudaKernel_t adj_kernel = nullptr;
     int adj_tape = 0;
     bool adj_analytic = false;
+    bool adj_fast_div = false;
     void *adj_scratch = nullptr;
     size_t adj_scratch_bytes = 0;
 
@@ -316,7 +317,7 @@ void sodecl_cfg_init(sodecl_cfg *cfg)
     cfg->fmad = 1;
     cfg->newton_tol = 1e-7;
     cfg->newton_max_iter = 1000;
-    cfg->division = SODECL_DIV_IEEE;
+    cfg->division = SODECL_DIV_RECIPROCAL;
 }
 
 int sodecl_cuda_abi_version(void) { return SODECL_CUDA_ABI_VERSION; }
@@ -829,11 +830,19 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     const long long per_wave = static_cast<long long>(std::max(1, sms)) * 128;
     const long long waves = (io->n + per_wave - 1) / per_wave;
     const int min_blocks = waves <= 2 ? 0 : static_cast<int>(std::min<long long>(4, waves));
-    if (!ctx->adj_prog || ctx->adj_tape != tape || ctx->adj_analytic != analytic || ctx->adj_min_blocks != min_blocks) {
+    // Division: loss-only passes (the forward sweep) follow the context's mode;
+    // passes with gradients use IEEE division, measured faster there (the
+    // reciprocal wrapper costs registers the backward sweep needs).  The
+    // quotients are the same either way.
+    const bool gradient = io->grad_params || io->grad_y0;
+    const bool fast_div = !gradient && ctx->cfg.division == SODECL_DIV_RECIPROCAL;
+    if (!ctx->adj_prog || ctx->adj_tape != tape || ctx->adj_analytic != analytic || ctx->adj_min_blocks != min_blocks ||
+        ctx->adj_fast_div != fast_div) {
         try {
             ProgramSpec spec = make_spec(ctx->cfg);
             spec.block_max = 128;
             spec.min_blocks = min_blocks;
+            spec.fast_div = fast_div;
             auto prog = sodecl_b200::build_adjoint(spec, ctx->system_src, tape, analytic);
             if (ctx->adj_lib) cudaLibraryUnload(ctx->adj_lib);
             ctx->adj_lib = nullptr;
@@ -842,6 +851,7 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
             ctx->adj_tape = tape;
             ctx->adj_analytic = analytic;
             ctx->adj_min_blocks = min_blocks;
+            ctx->adj_fast_div = fast_div;
         } catch (const std::exception &ex) {
             return ctx->fail(SODECL_ERR_COMPILE, ex.what());
         }

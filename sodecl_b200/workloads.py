@@ -104,6 +104,8 @@ def _parse():
     ap.add_argument("--lanes", type=int, default=1)
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--precision", default="fp64")
+    ap.add_argument("--division", default="ieee", choices=["ieee", "reciprocal"])
+    ap.add_argument("--min-blocks", type=int, default=0)
     ap.add_argument("--launches", type=int, default=2)
     return ap.parse_args()
 
@@ -133,7 +135,8 @@ def main():
     else:
         raise SystemExit("unknown case " + a.case)
     sim = Integrator(system_path(system), solver, dt=dt, tspan=a.nsteps * dt, ksteps=a.ksteps, neq=neq,
-                     npar=p.shape[1], nnoi=nnoi, orbits=n, precision=a.precision, lanes=a.lanes, block=a.block)
+                     npar=p.shape[1], nnoi=nnoi, orbits=n, precision=a.precision, lanes=a.lanes, block=a.block,
+                     division=a.division, min_blocks=a.min_blocks)
     dev = torch.device("cuda", 0)
     stream = torch.cuda.current_stream(dev)
     T = lambda x: torch.tensor(x, device=dev)  # noqa: E731
@@ -152,7 +155,8 @@ def main():
         torch.cuda.synchronize()
         ms = s.elapsed_time(e)
         print(json.dumps({"case": a.case, "launch": k, "ms": ms, "orbit_steps_per_s": n * a.nsteps / (ms * 1e-3),
-                          "lanes": a.lanes, "block": a.block or 128, "orbits": n, "nsteps": a.nsteps}), flush=True)
+                          "lanes": a.lanes, "block": a.block or 128, "orbits": n, "nsteps": a.nsteps,
+                          "division": sim.division, "min_blocks": a.min_blocks}), flush=True)
     sim.close()
 
 

@@ -203,7 +203,8 @@ def test_division_modes_and_fallback():
     needs plain double (an implicit conversion) falls back to IEEE division."""
     kw = dict(dt=1e-3, tspan=0.1, ksteps=10, neq=6, npar=6, orbits=4)
     assert Integrator(system_path("oculomotor"), "rk4", division="reciprocal", **kw).division == "reciprocal"
-    assert Integrator(system_path("oculomotor"), "rk4", **kw).division == "ieee"
+    assert Integrator(system_path("oculomotor"), "rk4", **kw).division == "reciprocal"  # the default
+    assert Integrator(system_path("oculomotor"), "rk4", division="ieee", **kw).division == "ieee"
     assert Integrator(system_path("oculomotor"), "rk4", division="reciprocal", precision="fp32", **kw).division == "ieee"
     src = open(system_path("oculomotor")).read().replace("double drive = y[3] - y[4];", "float drive = y[3] - y[4];")
     sim = Integrator(None, "rk4", system_src=src, division="reciprocal", **kw)

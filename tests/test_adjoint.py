@@ -172,8 +172,9 @@ def test_system_jacobians_match_central_differences(tmp_path, system, neq, npar,
 @pytest.mark.gpu
 @pytest.mark.parametrize("use_tape", [False, True])
 def test_adjoint_division_modes_bit_identical(use_tape):
-    """The reciprocal quotient gives IEEE-rounded results, so the adjoint built
-    with it returns the same bits."""
+    """Loss-only passes divide in the context's mode, passes with gradients in
+    IEEE division; the reciprocal quotient is IEEE-rounded, so losses and
+    gradients agree bit for bit across modes and passes."""
     torch = pytest.importorskip("torch")
     from sodecl_b200 import Integrator, system_path
     from sodecl_b200.fit import Adjoint
@@ -182,7 +183,12 @@ def test_adjoint_division_modes_bit_identical(use_tape):
     t0, y0, p, tg = fitting_problem(n, 4, dt=dt, nchunks=nchunks, ksteps=ksteps)
     kw = dict(dt=dt, tspan=(nchunks * ksteps - 0.5) * dt, ksteps=ksteps, neq=6, npar=6, orbits=n)
     T = lambda a: torch.tensor(a, device="cuda")  # noqa: E731
-    out = [Adjoint(Integrator(system_path("oculomotor"), "rk4", division=d, **kw), use_tape=use_tape)(
-        T(t0), T(y0), T(p), T(tg)) for d in ("ieee", "reciprocal")]
-    for a, b in zip(out[0][:3], out[1][:3]):
+    outs = []
+    for d in ("ieee", "reciprocal"):
+        adj = Adjoint(Integrator(system_path("oculomotor"), "rk4", division=d, **kw), use_tape=use_tape)
+        full = adj(T(t0), T(y0), T(p), T(tg))
+        loss_only = adj(T(t0), T(y0), T(p), T(tg), with_gradient=False)
+        assert torch.equal(full[0], loss_only[0])
+        outs.append(full)
+    for a, b in zip(outs[0][:3], outs[1][:3]):
         assert torch.equal(a, b)

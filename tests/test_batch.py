@@ -98,6 +98,12 @@ def single_kernel_final_state(system, solver, neq, npar, nnoi, dt, nsteps, t0, y
 @pytest.mark.gpu
 @pytest.mark.parametrize("fmad", [False, True])
 def test_batch_matches_single_system_kernel_bit_for_bit(fmad):
+    """Without FMA contraction both kernels evaluate every operation as
+    written, so the states agree bit for bit.  With contraction (fmad=1) the
+    compiler chooses which products to fuse separately in the two programs, so
+    last-bit differences may appear and grow over the steps: there the states
+    agree to 1e-9 relative (the parity tolerance of these step counts), the
+    times and draw counters exactly."""
     n = 3000
     cls, nsteps, t0, y0, p, counters = make_items(n, 1)
     b = make_batch(fmad)
@@ -109,7 +115,10 @@ def test_batch_matches_single_system_kernel_bit_for_bit(fmad):
         system, solver, neq, npar, nnoi, dt = CLASSES[cls[i]]
         tt, yy, cc = single_kernel_final_state(system, solver, neq, npar, nnoi, dt, nsteps[i], t0[i], y0[i], p[i],
                                                counters[i], i, fmad)
-        np.testing.assert_array_equal(y[i], yy)
+        if fmad:
+            np.testing.assert_allclose(y[i], yy, rtol=1e-9, atol=1e-12 * np.abs(yy).max())
+        else:
+            np.testing.assert_array_equal(y[i], yy)
         assert t[i] == tt
         if nnoi:
             assert cnt[i] == cc
