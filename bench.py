@@ -357,6 +357,9 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
     T = lambda x: torch.tensor(x, device=dev)  # noqa: E731
     adj = Adjoint(sim)
     adj_tape = Adjoint(sim, use_tape=True)
+    # the same file without calc_vjp: products from calc_jacobian + calc_jacobian_params
+    src = open(system_path("oculomotor")).read().replace("void calc_vjp(", "void unused_calc_vjp(")
+    adj_jac = Adjoint(Integrator(None, "rk4", orbits=n, system_src=src, **kw))
     wide = Adjoint(Integrator(system_path("oculomotor"), "rk4", orbits=n * 24, **kw))
     t0, y0d, gd = T(np.zeros(n)), T(y0), T(guess)
 
@@ -374,6 +377,7 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
         return float(np.median(out)), r
 
     ms_adj, (loss, gp, gy, flags) = timed(lambda: adj(t0, y0d, gd, targets))
+    ms_jac, (_, gpj, _, _) = timed(lambda: adj_jac(t0, y0d, gd, targets))
     ms_tape, (_, gpt, gyt, _) = timed(lambda: adj_tape(t0, y0d, gd, targets), reps=1)
     ms_fd, (fp, fy) = timed(lambda: finite_difference_gradient(t0, y0d, gd, targets, wide))
     ms_fwd, _ = timed(lambda: adj(t0, y0d, gd, targets, with_gradient=False))
@@ -383,16 +387,19 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
     dp = ((gp - fp).abs().amax(1) / gp.abs().amax(1)).cpu().numpy()
     dy = ((gy - fy).abs().amax(1) / gy.abs().amax(1)).cpu().numpy()
     err_tape = ((gpt - gp).abs().amax(1) / gp.abs().amax(1)).max().item()
+    err_jac = ((gpj - gp).abs().amax(1) / gp.abs().amax(1)).max().item()
     q = lambda d: {"median": float(np.median(d)), "p99": float(np.quantile(d, 0.99)),  # noqa: E731
                    "max": float(d.max()), "orbits_above_1e-4": int((d > 1e-4).sum())}
     return {"orbits": n, "nsteps": nsteps, "record_every": ksteps, "dt": dt, "adjoint_ms": ms_adj,
             "division": "IEEE in the gradient pass, reciprocal in loss-only passes (finite differences, loss_only)",
-            "adjoint_tape_ms": ms_tape, "rel_diff_tape_vs_analytic": err_tape,
+            "adjoint_jacobians_ms": ms_jac, "adjoint_tape_ms": ms_tape,
+            "rel_diff_jacobians_vs_vjp": err_jac, "rel_diff_tape_vs_vjp": err_tape,
             "finite_difference_ms": ms_fd, "loss_only_ms": ms_fwd, "speedup_vs_fd": ms_fd / ms_adj,
             "rel_diff_vs_fd_params": q(dp), "rel_diff_vs_fd_y0": q(dy),
             "tape_overflow": int((flags != 0).sum().item()),
             "fd": "central, relative step 1e-6, 24 perturbed copies per orbit in one launch",
-            "derivatives": "calc_jacobian + calc_jacobian_params of the system file; tape: reverse mode over sode_system"}
+            "derivatives": "adjoint_ms: the system file's calc_vjp; adjoint_jacobians_ms: its calc_jacobian + "
+                           "calc_jacobian_params; adjoint_tape_ms: reverse mode over sode_system"}
 
 
 def batch_lanes(system, neq):

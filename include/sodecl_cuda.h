@@ -222,8 +222,10 @@ typedef struct sodecl_adjoint_io {
     int32_t ckpt_every;     /* steps per checkpoint; 0 = ceil(sqrt(steps)) */
     int32_t tape_entries;   /* operations one right-hand side may record; 0 = 256 */
     int32_t use_tape;       /* 1: differentiate sode_system on the tape even when the system file
-                               provides calc_jacobian and calc_jacobian_params (df/dp, optional
-                               addition to the system-file interface), which are used otherwise */
+                               provides the products itself -- calc_vjp(t, y, v, ybar, pbar, p)
+                               (ybar += v^T df/dy, pbar += v^T df/dp), else calc_jacobian with
+                               calc_jacobian_params (df/dp): optional additions to the
+                               system-file interface, used in that order otherwise */
 } sodecl_adjoint_io;
 
 #define SODECL_FLAG_TAPE_OVERFLOW 4

@@ -55,6 +55,10 @@ inline Dual operator+(const Dual &a) { return a; }
     inline Dual operator op(const Dual &a, int b) { return a op Dual(b); }    \
     inline Dual operator op(int a, const Dual &b) { return Dual(a) op b; }
 DUAL_MIXED(+) DUAL_MIXED(-) DUAL_MIXED(*) DUAL_MIXED(/)
+inline Dual &operator+=(Dual &a, const Dual &b) { return a = a + b; }
+inline Dual &operator-=(Dual &a, const Dual &b) { return a = a - b; }
+inline Dual &operator*=(Dual &a, const Dual &b) { return a = a * b; }
+inline Dual &operator/=(Dual &a, const Dual &b) { return a = a / b; }
 #define DUAL_CMP(op)                                                              \
     inline bool operator op(const Dual &a, const Dual &b) { return a.v op b.v; }  \
     inline bool operator op(const Dual &a, double b) { return a.v op b; }         \

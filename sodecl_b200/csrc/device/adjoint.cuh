@@ -20,10 +20,13 @@
 // Part 2 (SODECL_ADJOINT_KERNEL, after both copies of the user file): the
 // step adjoints and the kernel.
 //
-// When the system file provides both calc_jacobian (df/dy, as the implicit
-// solvers use it) and calc_jacobian_params (df/dp), the products come from
-// them instead (SODECL_ADJ_ANALYTIC): no tape, all in registers -- the fast
-// path; the tape serves every other system file.
+// Where the products come from (SODECL_ADJ_MODE):
+//   2  the system file's calc_vjp(t, y, v, ybar, pbar, p), which accumulates
+//      v^T df/dy and v^T df/dp itself (only the nonzero terms, shared
+//      subexpressions): the fastest;
+//   1  its calc_jacobian (df/dy, as the implicit solvers use it) and
+//      calc_jacobian_params (df/dp): dense products in registers;
+//   0  the tape, for every other system file.
 
 #ifndef SODECL_ADJOINT_TYPES
 #define SODECL_ADJOINT_TYPES
@@ -173,7 +176,34 @@ __device__ __forceinline__ void sodecl_tape_sweep(const sodecl_tape &t, double *
 // Part 2.  Needs: the plain system (sode_system), the recording copy
 // (sodecl_adsys::sode_system), the solver step functions (solvers.cuh).
 
-#if SODECL_ADJ_ANALYTIC
+#if SODECL_ADJ_MODE == 2
+// For the seed v: xbar += v^T df/dx, pbar += v^T df/dp, by the system file's
+// own vector-Jacobian product.
+__device__ __forceinline__ void sodecl_vjp(double t, const double *x, const double *p, const double *v, double *xbar,
+                                           double *pbar, sodecl_tape *tape, double *adj, int &overflow)
+{
+    (void)tape;
+    (void)adj;
+    (void)overflow;
+    real_t xx[_numeq_], pp[SODECL_NPAR_ALLOC], vv[_numeq_], xb[_numeq_], pb[SODECL_NPAR_ALLOC];
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) {
+        xx[e] = (real_t)x[e];
+        vv[e] = (real_t)v[e];
+        xb[e] = (real_t)0;
+    }
+#pragma unroll SODECL_PAR_UNROLL
+    for (int j = 0; j < _numpar_; ++j) {
+        pp[j] = (real_t)p[j];
+        pb[j] = (real_t)0;
+    }
+    calc_vjp((real_t)t, xx, vv, xb, pb, pp);
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) xbar[e] += (double)xb[e];
+#pragma unroll SODECL_PAR_UNROLL
+    for (int j = 0; j < _numpar_; ++j) pbar[j] += (double)pb[j];
+}
+#elif SODECL_ADJ_MODE == 1
 // For the seed v: xbar += v^T df/dx, pbar += v^T df/dp, from the system
 // file's own Jacobians (calc_jacobian, calc_jacobian_params): two small
 // dense products, everything in registers.
@@ -338,7 +368,7 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
     if (!a.grad_p) return;
 
     // backward, segment by segment from the last
-#if SODECL_ADJ_ANALYTIC
+#if SODECL_ADJ_MODE != 0
     sodecl_tape *tape = nullptr;  // the analytic products record nothing
     double *adj = nullptr;
 #else

@@ -341,6 +341,7 @@ SystemTraits inspect_system(const std::string &src)
     t.has_row = defines_function(stripped, "sode_system_row");
     t.has_stoch_row = defines_function(stripped, "sode_system_stoch_row");
     t.has_jac_band = defines_function(stripped, "calc_jacobian_band");
+    t.has_vjp = defines_function(stripped, "calc_vjp");
     t.uses_listsize = std::regex_search(stripped, std::regex("\\b_listsize_\\b"));
     return t;
 }
@@ -544,7 +545,7 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
     return s.str();
 }
 
-std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, int tape_cap, bool analytic,
+std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, int tape_cap, int mode,
                              bool fast_div)
 {
     const SystemTraits tr = inspect_system(src);
@@ -559,7 +560,7 @@ std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, in
     s << "#define SODECL_BLOCK_MAX " << spec.block_max << "\n";
     if (spec.min_blocks > 0) s << "#define SODECL_MIN_BLOCKS " << spec.min_blocks << "\n";
     s << "#define SODECL_TAPE_CAP " << tape_cap << "\n";
-    s << "#define SODECL_ADJ_ANALYTIC " << (analytic ? 1 : 0) << "\n";
+    s << "#define SODECL_ADJ_MODE " << mode << "\n";
     s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n" << kAdjointSrc << "\n";
     s << "#define _numnoi_ " << spec.num_noi << "\n";
     s << "#define _listsize_ " << spec.list_size << "\n";
@@ -586,17 +587,17 @@ std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, in
 }  // namespace
 
 std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std::string &system_src, int tape_cap,
-                                             bool analytic)
+                                             int mode)
 {
     // the reciprocal quotients only where the system file is plain arithmetic
     if (spec.fast_div && system_src.find("printf") == std::string::npos) {
         try {
-            return compile_text(assemble_adjoint(spec, system_src, tape_cap, analytic, true), spec.fmad, true,
+            return compile_text(assemble_adjoint(spec, system_src, tape_cap, mode, true), spec.fmad, true,
                                 "sodecl_adjoint");
         } catch (const std::exception &) {
         }
     }
-    return compile_text(assemble_adjoint(spec, system_src, tape_cap, analytic, false), spec.fmad, false,
+    return compile_text(assemble_adjoint(spec, system_src, tape_cap, mode, false), spec.fmad, false,
                         "sodecl_adjoint");
 }
 

@@ -44,6 +44,7 @@ struct SystemTraits {
     bool has_row = false;        // sode_system_row (one equation's right-hand side)
     bool has_stoch_row = false;  // sode_system_stoch_row
     bool has_jac_band = false;   // calc_jacobian_band (row i's entries in columns i-1, i, i+1)
+    bool has_vjp = false;        // calc_vjp (v^T df/dy and v^T df/dp), used by the adjoint
     bool uses_listsize = false;
 };
 
@@ -70,10 +71,11 @@ std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string 
 
 // The discrete-adjoint program (kernel `sodecl_adjoint`) for the Euler or RK4
 // solver: the system file twice, plain and with `double` recording on a tape
-// of `tape_cap` entries per right-hand-side evaluation; with `analytic`, the
-// products come from the file's calc_jacobian and calc_jacobian_params.
+// of `tape_cap` entries per right-hand-side evaluation.  mode: where the
+// vector-Jacobian products come from -- 2 the file's calc_vjp, 1 its
+// calc_jacobian and calc_jacobian_params, 0 the tape.
 std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std::string &system_src, int tape_cap,
-                                             bool analytic);
+                                             int mode);
 
 // One class of a heterogeneous batch: a system file with a solver, sizes,
 // step and Newton settings (kernel_steps/list_size unused).

@@ -102,7 +102,7 @@ struct sodecl_ctx {
     cudaLibrary_t adj_lib = nullptr;
     cudaKernel_t adj_kernel = nullptr;
     int adj_tape = 0;
-    bool adj_analytic = false;
+    int adj_mode = -1;
     bool adj_fast_div = false;
     void *adj_scratch = nullptr;
     size_t adj_scratch_bytes = 0;
@@ -817,7 +817,8 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     DeviceScope dev(ctx->cfg.device);
     const int tape = io->tape_entries > 0 ? io->tape_entries : 256;
     const auto traits = sodecl_b200::inspect_system(ctx->system_src);
-    const bool analytic = !io->use_tape && traits.has_jacobian && traits.has_pjacobian;
+    // products: the file's calc_vjp, else its two Jacobians, else the tape
+    const int mode = io->use_tape ? 0 : traits.has_vjp ? 2 : (traits.has_jacobian && traits.has_pjacobian) ? 1 : 0;
     // Resident blocks the compiler must allow for (a register cap): enough
     // that every orbit gets a thread in the first wave, up to 4 blocks of 128
     // (128 registers).  Each thread runs its orbit's whole forward and
@@ -836,20 +837,20 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     // quotients are the same either way.
     const bool gradient = io->grad_params || io->grad_y0;
     const bool fast_div = !gradient && ctx->cfg.division == SODECL_DIV_RECIPROCAL;
-    if (!ctx->adj_prog || ctx->adj_tape != tape || ctx->adj_analytic != analytic || ctx->adj_min_blocks != min_blocks ||
+    if (!ctx->adj_prog || ctx->adj_tape != tape || ctx->adj_mode != mode || ctx->adj_min_blocks != min_blocks ||
         ctx->adj_fast_div != fast_div) {
         try {
             ProgramSpec spec = make_spec(ctx->cfg);
             spec.block_max = 128;
             spec.min_blocks = min_blocks;
             spec.fast_div = fast_div;
-            auto prog = sodecl_b200::build_adjoint(spec, ctx->system_src, tape, analytic);
+            auto prog = sodecl_b200::build_adjoint(spec, ctx->system_src, tape, mode);
             if (ctx->adj_lib) cudaLibraryUnload(ctx->adj_lib);
             ctx->adj_lib = nullptr;
             ctx->adj_kernel = nullptr;
             ctx->adj_prog = prog;
             ctx->adj_tape = tape;
-            ctx->adj_analytic = analytic;
+            ctx->adj_mode = mode;
             ctx->adj_min_blocks = min_blocks;
             ctx->adj_fast_div = fast_div;
         } catch (const std::exception &ex) {

@@ -21,7 +21,8 @@
  * argument instead of branching (same values, see there); jac[4][5] carries the
  * chain-rule sign the reference's calc_jacobian omits (entries off the three
  * bands are never read by the implicit solvers), and calc_jacobian_params
- * (df/dp, for the adjoint) is an addition.
+ * (df/dp) and calc_vjp (the vector-Jacobian product), both for the adjoint,
+ * are additions.
  */
 
 #define OCM_T1 0.15
@@ -156,6 +157,54 @@ void calc_jacobian_params(double y[_numeq_], double jacp[_numeq_][_numpar_], dou
 	jacp[4][3] = -(y[4] * y[3] * y[3]) * itau;
 	jacp[4][4] = dl[2] * itau;
 	jacp[4][5] = dl[3] * itau;
+}
+
+/* ocm_burst and its slope and parameter derivatives with one exp:
+ * d = [dB/dx, dB/da, dB/db, dB/dat, dB/dbt] */
+double ocm_burst_all(double x, double a, double b, double at, double bt, double d[5])
+{
+	int right = x > 0;
+	double e = exp(x / (right ? -bt : b));
+	double ib = 1.00 / b;
+	double ibt = 1.00 / bt;
+	double g = 1.00 + x * ib;
+	d[0] = right ? at * e * ibt : -(a * ib) * e * g;
+	d[1] = right ? (double)0 : -(x * e) * ib;
+	d[2] = right ? (double)0 : (a * x * e) * ib * ib * g;
+	d[3] = right ? 1.00 - e : (double)0;
+	d[4] = right ? -(at * x * e) * ibt * ibt : (double)0;
+	return right ? (at * (1.00 - e)) : (-(a * ib) * x * e);
+}
+
+/* ybar[j] += sum_i v[i] d yout[i] / d y[j], pbar[k] += sum_i v[i] d yout[i] / d p[k]
+ * for the six model parameters: the vector-Jacobian product of sode_system,
+ * term by term (not in the reference's file; the adjoint uses it in place of
+ * calc_jacobian and calc_jacobian_params) */
+void calc_vjp(double t, double y[_numeq_], double v[_numeq_], double ybar[_numeq_], double pbar[_numpar_],
+              double p[_numpar_])
+{
+	double itau = 1.00 / p[2];
+	double dr[5], dl[5];
+	double br = ocm_burst_all(y[5], p[0], p[1], p[4], p[5], dr);
+	double bl = ocm_burst_all(-y[5], p[0], p[1], p[4], p[5], dl);
+	double wr = v[3] * itau;
+	double wl = v[4] * itau;
+	/* drive = y3 - y4 enters yout1 (gain VEL), yout2 (1) and yout5 (-1) */
+	double vdrive = v[1] * OCM_VEL_GAIN + v[2] - v[5];
+	ybar[0] += -(v[1] * OCM_POS_GAIN);
+	ybar[1] += v[0] - v[1] * OCM_VEL_GAIN;
+	ybar[2] += v[1] * OCM_POS_GAIN - v[2] / OCM_TN;
+	ybar[3] += vdrive + wr * (-1.00 - p[3] * y[4] * y[4]) + wl * (-2.00 * p[3] * y[4] * y[3]);
+	ybar[4] += -vdrive + wr * (-2.00 * p[3] * y[3] * y[4]) + wl * (-1.00 - p[3] * y[3] * y[3]);
+	ybar[5] += wr * dr[0] - wl * dl[0];
+	double r = -y[3] - (p[3] * y[3] * y[4] * y[4]) + br;
+	double l = -y[4] - (p[3] * y[4] * y[3] * y[3]) + bl;
+	pbar[0] += wr * dr[1] + wl * dl[1];
+	pbar[1] += wr * dr[2] + wl * dl[2];
+	pbar[2] += -(wr * r + wl * l) * itau;
+	pbar[3] += -(wr * y[3] * y[4] * y[4] + wl * y[4] * y[3] * y[3]);
+	pbar[4] += wr * dr[3] + wl * dl[3];
+	pbar[5] += wr * dr[4] + wl * dl[4];
 }
 
 void sode_system_stoch(double t, double y[_numeq_], double stoch[_numeq_], double p[_numpar_], double noise[_numnoi_])

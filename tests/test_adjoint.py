@@ -8,8 +8,9 @@ The GPU adjoint (sodecl_cuda_adjoint) is checked against
   * central finite differences of the GPU loss (relative step 1e-6), the
     baseline the adjoint replaces -- agreement to 1e-5, the finite differences'
     own error at that step being a few 1e-6.
-Both derivative paths are exercised: the system file's analytic Jacobians
-(calc_jacobian + calc_jacobian_params) and the reverse-mode tape.
+All three derivative paths are exercised: the system file's own
+vector-Jacobian product (calc_vjp), its analytic Jacobians (calc_jacobian +
+calc_jacobian_params), and the reverse-mode tape.
 The per-orbit loss is checked against the CPU oracle's records."""
 import os
 
@@ -56,21 +57,35 @@ def test_reference_gradient_matches_cpu_finite_differences():
         assert np.allclose(fd, gp[:, j], rtol=1e-5, atol=1e-9 * np.abs(gp).max())
 
 
+def oculomotor_source(products):
+    """The oculomotor system file with the adjoint taking `products` from
+    calc_vjp ("vjp"), from the two Jacobians ("jacobians": calc_vjp renamed
+    away) or from the tape ("tape")."""
+    from sodecl_b200 import system_path
+
+    src = open(system_path("oculomotor")).read()
+    if products == "jacobians":
+        src = src.replace("void calc_vjp(", "void unused_calc_vjp(")
+    return src
+
+
 @pytest.mark.gpu
-@pytest.mark.parametrize("use_tape", [False, True])
+@pytest.mark.parametrize("products", ["vjp", "jacobians", "tape"])
 @pytest.mark.parametrize("solver", ["rk4", "euler"])
-def test_adjoint_matches_reference_gradient(solver, use_tape):
+def test_adjoint_matches_reference_gradient(solver, products):
     torch = pytest.importorskip("torch")
     from sodecl_b200 import Integrator, system_path
     from sodecl_b200.fit import Adjoint
+
+    use_tape = products == "tape"
 
     n, nchunks, ksteps, dt = 64, 10, 50, 1e-5 if solver == "rk4" else 1e-6
     t0, y0, p, tg = fitting_problem(n, 1, dt=dt, nchunks=nchunks, ksteps=ksteps)
     sid = 2 if solver == "rk4" else 1
     loss_r, gp_r, gy_r = reference_gradient(system_path("oculomotor"), sid, 6, 6, dt, ksteps, nchunks, t0[:8], y0[:8],
                                             p[:8], tg[:, :, :8])
-    sim = Integrator(system_path("oculomotor"), solver, dt=dt, tspan=(nchunks * ksteps - 0.5) * dt, ksteps=ksteps,
-                     neq=6, npar=6, orbits=n)
+    sim = Integrator(None, solver, dt=dt, tspan=(nchunks * ksteps - 0.5) * dt, ksteps=ksteps,
+                     neq=6, npar=6, orbits=n, system_src=oculomotor_source(products))
     assert sim.num_chunks == nchunks
     dev = torch.device("cuda")
     T = lambda a: torch.tensor(a, device=dev)  # noqa: E731
@@ -138,9 +153,9 @@ def test_torch_autograd_function_and_tape_overflow():
 
 @pytest.mark.parametrize("system,neq,npar,jacp", [("oculomotor", 6, 6, True), ("kuramoto", 8, 9, False)])
 def test_system_jacobians_match_central_differences(tmp_path, system, neq, npar, jacp):
-    """calc_jacobian (and calc_jacobian_params where present) against central
-    differences of sode_system, on the host.  Both bursts' branches of the
-    oculomotor model are visited (y5 of either sign)."""
+    """calc_jacobian (and calc_jacobian_params and calc_vjp where present)
+    against central differences of sode_system, on the host.  Both bursts'
+    branches of the oculomotor model are visited (y5 of either sign)."""
     import subprocess
 
     exe = str(tmp_path / "jacobian_fd")
@@ -148,7 +163,7 @@ def test_system_jacobians_match_central_differences(tmp_path, system, neq, npar,
            '-DSYSTEM_FILE="%s"' % os.path.join(SYSTEMS, system + ".cl"),
            os.path.join(REPO, "tests", "cpp", "jacobian_fd.cpp"), "-o", exe]
     if jacp:
-        cmd.insert(1, "-DHAS_JACP")
+        cmd[1:1] = ["-DHAS_JACP", "-DHAS_VJP"]
     subprocess.run(cmd, check=True)
     rng = np.random.default_rng(7)
     cases = []
@@ -163,10 +178,10 @@ def test_system_jacobians_match_central_differences(tmp_path, system, neq, npar,
         cases.append(" ".join("%.17g" % v for v in np.concatenate([y, p])))
     out = subprocess.run([exe], input="\n".join(cases) + "\n", capture_output=True, text=True, check=True).stdout
     errs = np.array([[float(v) for v in line.split()] for line in out.strip().splitlines()])
-    assert errs.shape == (16, 2)
-    print("%s: max rel diff J %.2e, Jp %.2e" % (system, errs[:, 0].max(), errs[:, 1].max()))
-    assert errs[:, 0].max() < 1e-5
-    assert errs[:, 1].max() < 1e-5
+    assert errs.shape == (16, 3)
+    print("%s: max rel diff J %.2e, Jp %.2e, vjp %.2e" % (system, errs[:, 0].max(), errs[:, 1].max(),
+                                                          errs[:, 2].max()))
+    assert errs.max() < 1e-5
 
 
 @pytest.mark.gpu
