@@ -202,10 +202,16 @@ int sodecl_cuda_launch(sodecl_ctx *ctx, const sodecl_launch *launch, void *strea
  * For every orbit, the mean squared error of its records against targets,
  *   loss_i = sum_{r,e} (y_{r,e,i} - target_{r,e,i})^2 / (records * num_equat),
  * and (optionally) its gradient with respect to the orbit's parameters and
- * initial state, by the discrete adjoint of the Euler or RK4 steps (FP64):
- * the user's right-hand side differentiated in reverse mode (the system file
- * compiled a second time with a recording `double`), the state checkpointed
- * every `ckpt_every` steps (0: ~sqrt(steps)) and recomputed per segment.
+ * initial state, by the discrete adjoint of the steps (FP64): of the Euler
+ * and RK4 arithmetic, and of the implicit Euler / midpoint steps taken as
+ * solved exactly (a transposed solve with calc_jacobian's full matrix per
+ * step; the forward Newton passes stop at newton_tol, so the gradient is that
+ * of the exact implicit step, closer the tighter the tolerance).  The
+ * vector-Jacobian products come from the system file's calc_vjp, else its
+ * calc_jacobian + calc_jacobian_params, else the right-hand side
+ * differentiated in reverse mode (the system file compiled a second time
+ * with a recording `double`).  The state is checkpointed every `ckpt_every`
+ * steps (0: ~sqrt(steps)) and recomputed per segment.
  * Records, steps and the step size follow the context's configuration; all
  * pointers are device pointers; the launch goes on `stream`.  No
  * counterpart in the reference. */
@@ -217,7 +223,8 @@ typedef struct sodecl_adjoint_io {
     double *loss;           /* [n] out */
     double *grad_params;    /* [n][num_params] out, or NULL for the loss alone */
     double *grad_y0;        /* [n][num_equat] out, or NULL */
-    int32_t *flags;         /* [n] out, or NULL: 4 = tape overflow (raise tape_entries) */
+    int32_t *flags;         /* [n] out, or NULL: 4 = tape overflow (raise tape_entries),
+                               1 = a Newton step stopped at newton_max_iter */
     int64_t n;              /* orbits, <= list_size */
     int32_t ckpt_every;     /* steps per checkpoint; 0 = ceil(sqrt(steps)) */
     int32_t tape_entries;   /* operations one right-hand side may record; 0 = 256 */

@@ -3,11 +3,12 @@
 // FP64 reference gradient for the discrete adjoint: forward-mode dual numbers
 // (value + NUMPAR + NUMEQ tangents) pushed through the system file and a
 // restatement of the Euler / RK4 steps (src/kernels/euler.cl:10-18,
-// rk4.cl:17-64, same evaluation order).  Exact to rounding; slow, so the
-// tests use a few orbits.
+// rk4.cl:17-64, same evaluation order) and of the implicit Euler / midpoint
+// Newton passes (ie.cl, im.cl).  Exact to rounding; slow, so the tests use a
+// few orbits.
 //
 // Build: g++ -O2 -std=c++17 -DSYSTEM_FILE='"x.cl"' -DNUMEQ=6 -DNUMPAR=6 gradient.cpp
-// Run:   gradient <solver 1|2> <in.bin> <out.bin>
+// Run:   gradient <solver 1|2|3|4> <in.bin> <out.bin> [<newton tol> <newton pass limit>]
 //   in:  int64 n, nchunks, ksteps; double dt; t0[n]; y0[n][neq]; p[n][npar];
 //        targets[nchunks+1][neq][n]
 //   out: loss[n]; grad_p[n][npar]; grad_y0[n][neq]
@@ -110,10 +111,67 @@ static void step_rk4(double h, const T &t, const T *y, T *ynew, T *p)
     for (int e = 0; e < NUMEQ; ++e) ynew[e] = y[e] + (ynew[e] + stage[e]) * h / 6.00;
 }
 
+// The implicit solvers as the reference runs them (src/kernels/ie.cl:10-117,
+// im.cl:3-118): quasi-Newton passes with the banded solve, stopping at the
+// residual bound; dual numbers carry the derivatives through every pass.
+static double g_newton_tol = 1e-7;
+static long long g_newton_max = 1000;
+
+static void band_solve(T (*m)[NUMEQ], T *v, T *x)
+{
+    T up[NUMEQ], lo[NUMEQ], d[NUMEQ];
+    for (int i = 0; i < NUMEQ; ++i) {
+        up[i] = (i < NUMEQ - 2) ? m[i][(i + 1) % NUMEQ] : T(0.0);
+        lo[i] = (i < NUMEQ - 1) ? m[(i + 1) % NUMEQ][i] : T(0.0);
+        d[i] = m[i][i];
+    }
+    for (int i = 1; i < NUMEQ; ++i) {
+        const T f = up[i] / d[i - 1];
+        d[i] = d[i] - f * lo[i - 1];
+        v[i] = v[i] - f * v[i - 1];
+    }
+    x[NUMEQ - 1] = v[NUMEQ - 1] / d[NUMEQ - 1];
+    for (int i = NUMEQ - 2; i >= 0; --i) x[i] = (v[i] - lo[i] * x[i + 1]) / d[i];
+}
+
+static void step_implicit(bool midpoint, double h, const T &t, const T *y, T *ynew, T *p)
+{
+    T x[NUMEQ], f[NUMEQ], r[NUMEQ], dx[NUMEQ], mid[NUMEQ], m[NUMEQ][NUMEQ];
+    for (int e = 0; e < NUMEQ; ++e) x[e] = y[e];
+    for (long long pass = 0; pass < g_newton_max; ++pass) {
+        if (midpoint) {
+            for (int e = 0; e < NUMEQ; ++e) mid[e] = (y[e] + x[e]) * 0.5;
+            sode_system(t, mid, f, p);
+        } else {
+            sode_system(t, x, f, p);
+        }
+        T norm(0.0);
+        for (int e = 0; e < NUMEQ; ++e) {
+            r[e] = x[e] - y[e] - f[e] * h;
+            norm = midpoint ? norm + r[e] * r[e] : norm + fabs(r[e]);
+        }
+        if ((midpoint ? sqrt(norm).v : norm.v) < g_newton_tol) break;
+        calc_jacobian(midpoint ? mid : x, m, p);
+        const double scale = midpoint ? -0.50 : -1.00;
+        for (int i = 0; i < NUMEQ; ++i) {
+            for (int j = 0; j < NUMEQ; ++j) m[i][j] = m[i][j] * scale * h;
+            m[i][i] = m[i][i] + 1;
+        }
+        band_solve(m, r, dx);
+        for (int e = 0; e < NUMEQ; ++e) x[e] = x[e] - dx[e];
+    }
+    for (int e = 0; e < NUMEQ; ++e) ynew[e] = x[e];
+}
+
 int main(int argc, char **argv)
 {
-    if (argc != 4) return 2;
+    // argv: solver, input file, output file [, Newton tolerance, Newton pass limit]
+    if (argc != 4 && argc != 6) return 2;
     const int solver = std::atoi(argv[1]);
+    if (argc == 6) {
+        g_newton_tol = std::atof(argv[4]);
+        g_newton_max = std::atoll(argv[5]);
+    }
     FILE *in = std::fopen(argv[2], "rb");
     if (!in) return 3;
     long long hdr[3];
@@ -141,7 +199,8 @@ int main(int argc, char **argv)
             if (r == nchunks) break;
             for (long long s = 0; s < ksteps; ++s) {
                 if (solver == 1) step_euler(dt, t, y, ynew, pp);
-                else step_rk4(dt, t, y, ynew, pp);
+                else if (solver == 2) step_rk4(dt, t, y, ynew, pp);
+                else step_implicit(solver == 4, dt, t, y, ynew, pp);
                 t = t + dt;
                 for (int e = 0; e < NUMEQ; ++e) y[e] = ynew[e];
             }

@@ -186,10 +186,12 @@ def to_reference_layout(records: np.ndarray) -> np.ndarray:
     return records.reshape(nrec, -1).T.copy()
 
 
-def reference_gradient(system_file, solver, neq, npar, dt, ksteps, nchunks, t0, y0, params, targets):
+def reference_gradient(system_file, solver, neq, npar, dt, ksteps, nchunks, t0, y0, params, targets,
+                       newton_tol=1e-7, newton_max_iter=1000):
     """(loss[n], grad_params[n,npar], grad_y0[n,neq]) of the per-orbit MSE by
     forward-mode dual numbers through the system file (oracle/gradient.cpp),
-    stepping with printed_dt(dt)."""
+    stepping with printed_dt(dt); the implicit solvers (3, 4) stop their
+    Newton passes at printed_dt(newton_tol) or newton_max_iter passes."""
     import hashlib
     import subprocess
     import tempfile
@@ -212,6 +214,7 @@ def reference_gradient(system_file, solver, neq, npar, dt, ksteps, nchunks, t0, 
             f.write(np.array([printed_dt(dt)], dtype=np.float64).tobytes())
             for a in (t0, y0, params, targets):
                 f.write(np.ascontiguousarray(a, dtype=np.float64).tobytes())
-        subprocess.run([exe, str(solver), fin, fout], check=True)
+        subprocess.run([exe, str(solver), fin, fout, repr(printed_dt(newton_tol)), str(int(newton_max_iter))],
+                       check=True)
         out = np.fromfile(fout)
     return out[:n], out[n:n + n * npar].reshape(n, npar), out[n + n * npar:].reshape(n, neq)

@@ -251,13 +251,67 @@ __device__ __forceinline__ void sodecl_vjp(double t, const double *x, const doub
 }
 #endif
 
-// lambda <- (d step / d y)^T lambda, pbar += (d step / d p)^T lambda, for the
-// step taken from (t, y) with step h: the adjoint of sodecl_step_euler /
-// sodecl_step_rk4's arithmetic.
-__device__ __forceinline__ void sodecl_step_adjoint(double h, double t, const double *y, const double *p,
-                                                    double *lambda, double *pbar, sodecl_tape *tape, double *adj,
-                                                    int &overflow)
+#if SODECL_SOLVER == 3 || SODECL_SOLVER == 4
+// mu <- A^{-T} mu for A = I - c J (J row-major, _numeq_ x _numeq_): Gaussian
+// elimination with partial pivoting on A^T.  Row swaps are written as
+// selects over the rows below the pivot, so small systems stay in registers.
+__device__ __forceinline__ void sodecl_transposed_solve(const real_t (*J)[_numeq_], double c, double *mu)
 {
+    double a[_numeq_][_numeq_];
+#pragma unroll SODECL_EQ_UNROLL
+    for (int i = 0; i < _numeq_; ++i)
+#pragma unroll SODECL_EQ_UNROLL
+        for (int j = 0; j < _numeq_; ++j) a[i][j] = (i == j ? 1.0 : 0.0) - c * (double)J[j][i];
+#pragma unroll SODECL_EQ_UNROLL
+    for (int k = 0; k < _numeq_; ++k) {
+        int piv = k;
+        double best = fabs(a[k][k]);
+#pragma unroll SODECL_EQ_UNROLL
+        for (int i = k + 1; i < _numeq_; ++i)
+            if (fabs(a[i][k]) > best) {
+                best = fabs(a[i][k]);
+                piv = i;
+            }
+#pragma unroll SODECL_EQ_UNROLL
+        for (int i = k + 1; i < _numeq_; ++i) {
+            const bool sw = i == piv;
+#pragma unroll SODECL_EQ_UNROLL
+            for (int j = k; j < _numeq_; ++j) {
+                const double u = a[k][j];
+                a[k][j] = sw ? a[i][j] : u;
+                a[i][j] = sw ? u : a[i][j];
+            }
+            const double u = mu[k];
+            mu[k] = sw ? mu[i] : u;
+            mu[i] = sw ? u : mu[i];
+        }
+#pragma unroll SODECL_EQ_UNROLL
+        for (int i = k + 1; i < _numeq_; ++i) {
+            const double f = a[i][k] / a[k][k];
+#pragma unroll SODECL_EQ_UNROLL
+            for (int j = k + 1; j < _numeq_; ++j) a[i][j] -= f * a[k][j];
+            mu[i] -= f * mu[k];
+        }
+    }
+#pragma unroll SODECL_EQ_UNROLL
+    for (int k = _numeq_ - 1; k >= 0; --k) {
+        double sum = mu[k];
+#pragma unroll SODECL_EQ_UNROLL
+        for (int j = k + 1; j < _numeq_; ++j) sum -= a[k][j] * mu[j];
+        mu[k] = sum / a[k][k];
+    }
+}
+#endif
+
+// lambda <- (d step / d y)^T lambda, pbar += (d step / d p)^T lambda, for the
+// step taken from (t, y) to ynext with step h: the adjoint of
+// sodecl_step_euler / sodecl_step_rk4's arithmetic, and of the implicit steps
+// taken as solved exactly.
+__device__ __forceinline__ void sodecl_step_adjoint(double h, double t, const double *y, const double *ynext,
+                                                    const double *p, double *lambda, double *pbar, sodecl_tape *tape,
+                                                    double *adj, int &overflow)
+{
+    (void)ynext;
 #if SODECL_SOLVER == 1
     // y1 = y + h f(t, y)
     double seed[_numeq_], ybar[_numeq_];
@@ -304,8 +358,55 @@ __device__ __forceinline__ void sodecl_step_adjoint(double h, double t, const do
     for (int e = 0; e < _numeq_; ++e) xbar[e] = 0.0;
     sodecl_vjp(t, y, pv, kbar, xbar, pbar, tape, adj, overflow);
     for (int e = 0; e < _numeq_; ++e) lambda[e] = ybar[e] + xbar[e];
+#elif SODECL_SOLVER == 3 || SODECL_SOLVER == 4
+    // The implicit step taken as solved exactly (the Newton passes of
+    // src/kernels/ie.cl:50-117 / im.cl:43-118 stop at a residual bound; the
+    // gradient is that of the step they approximate):
+    //   IE: y1 = y + h f(t, y1):           (I - h J(y1)) dy1 = dy + h f_p dp
+    //   IM: y1 = y + h f(t, (y + y1)/2):   (I - h/2 J(m)) dy1 = (I + h/2 J(m)) dy + h f_p dp
+    // so mu = (I - c J)^{-T} lambda, lambda <- mu (IE) or mu + c J^T mu (IM),
+    // pbar += h f_p^T mu, with J from calc_jacobian (the full matrix: every
+    // entry counts here, unlike in the banded Newton solve).
+#if SODECL_SOLVER == 4
+    const double c = 0.5 * h;
 #else
-#error "the adjoint covers the Euler and RK4 solvers"
+    const double c = h;
+#endif
+    double x[_numeq_], mu[_numeq_];
+    real_t xx[_numeq_], pp[SODECL_NPAR_ALLOC], jj[_numeq_][_numeq_];
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) {
+#if SODECL_SOLVER == 4
+        x[e] = (y[e] + ynext[e]) * 0.5;
+#else
+        x[e] = ynext[e];
+#endif
+        xx[e] = (real_t)x[e];
+        mu[e] = lambda[e];
+    }
+#pragma unroll SODECL_PAR_UNROLL
+    for (int j = 0; j < _numpar_; ++j) pp[j] = (real_t)p[j];
+    calc_jacobian(xx, jj, pp);
+    sodecl_transposed_solve(jj, c, mu);
+    // J^T mu and f_p^T mu at x from the product source
+    double jtmu[_numeq_], fp[SODECL_NPAR_ALLOC];
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) jtmu[e] = 0.0;
+#pragma unroll SODECL_PAR_UNROLL
+    for (int j = 0; j < _numpar_; ++j) fp[j] = 0.0;
+    sodecl_vjp(t, x, p, mu, jtmu, fp, tape, adj, overflow);
+#pragma unroll SODECL_PAR_UNROLL
+    for (int j = 0; j < _numpar_; ++j) pbar[j] += h * fp[j];
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) {
+#if SODECL_SOLVER == 4
+        lambda[e] = mu[e] + c * jtmu[e];
+#else
+        lambda[e] = mu[e];
+#endif
+    }
+#else
+#error "the adjoint covers the Euler, RK4, implicit Euler and implicit midpoint solvers"
 #endif
 }
 
@@ -365,7 +466,10 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
         if (s < steps) sodecl_advance(t, y, p, i, counter, passes, capped);
     }
     a.loss[i] = loss * w;
-    if (!a.grad_p) return;
+    if (!a.grad_p) {
+        if (a.flags) a.flags[i] = capped ? SODECL_FLAG_NEWTON_CAP : 0;
+        return;
+    }
 
     // backward, segment by segment from the last
 #if SODECL_ADJ_MODE != 0
@@ -406,7 +510,8 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
             const long long c = s - s0;
             double ystep[_numeq_];
             for (int e = 0; e < _numeq_; ++e) ystep[e] = a.seg[(c * _numeq_ + e) * n + i];
-            sodecl_step_adjoint((double)_m_dt_, a.seg_t[c * n + i], ystep, pd, lambda, pbar, tape, adj, overflow);
+            sodecl_step_adjoint((double)_m_dt_, a.seg_t[c * n + i], ystep, ynext, pd, lambda, pbar, tape, adj,
+                                overflow);
             for (int e = 0; e < _numeq_; ++e) ynext[e] = ystep[e];
         }
     }
@@ -415,6 +520,6 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
     for (int j = 0; j < _numpar_; ++j) a.grad_p[i * _numpar_ + j] = pbar[j];
     if (a.grad_y0)
         for (int e = 0; e < _numeq_; ++e) a.grad_y0[i * _numeq_ + e] = lambda[e];
-    if (a.flags) a.flags[i] = overflow ? SODECL_FLAG_TAPE_OVERFLOW : 0;
+    if (a.flags) a.flags[i] = (overflow ? SODECL_FLAG_TAPE_OVERFLOW : 0) | (capped ? SODECL_FLAG_NEWTON_CAP : 0);
 }
 #endif  // SODECL_ADJOINT_KERNEL

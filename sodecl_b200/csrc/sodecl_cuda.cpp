@@ -807,8 +807,8 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     if (!ctx) return SODECL_ERR_INVALID_ARG;
     if (!io || !io->t0 || !io->y0 || (!io->params && ctx->cfg.num_params > 0) || !io->targets || !io->loss)
         return ctx->fail(SODECL_ERR_INVALID_ARG, "adjoint: t0, y0, params, targets and loss are required");
-    if (ctx->cfg.solver != SODECL_EULER && ctx->cfg.solver != SODECL_RUNGE_KUTTA)
-        return ctx->fail(SODECL_ERR_UNSUPPORTED, "the adjoint covers the Euler and RK4 solvers");
+    if (ctx->cfg.solver == SODECL_STOCHASTIC_EULER)
+        return ctx->fail(SODECL_ERR_UNSUPPORTED, "the adjoint covers the deterministic solvers");
     if (ctx->cfg.precision != SODECL_FP64) return ctx->fail(SODECL_ERR_UNSUPPORTED, "the adjoint is FP64");
     if (io->n < 1 || io->n > ctx->cfg.list_size) return ctx->fail(SODECL_ERR_INVALID_ARG, "adjoint: orbit count");
     if (io->tape_entries < 0 || io->tape_entries > 30000)

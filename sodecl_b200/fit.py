@@ -8,7 +8,8 @@
 
 Per orbit i, loss_i = sum_{r,e} (y_{r,e,i} - target_{r,e,i})^2 / (records * neq)
 over the records the integrator's configuration produces.  The gradient is the
-discrete adjoint of the Euler/RK4 steps (sodecl_cuda_adjoint), computed on the
+discrete adjoint of the Euler/RK4 steps, and of the implicit Euler/midpoint
+steps through their transposed Newton systems (sodecl_cuda_adjoint), computed on the
 GPU by one kernel; `finite_difference_gradient` is the central-difference
 baseline on the same GPU.
 """

@@ -25,12 +25,12 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SYSTEMS = os.path.join(REPO, "sodecl_b200", "systems")
 
 
-def fitting_problem(n, seed, dt=1e-5, nchunks=10, ksteps=50, noise=1e-2):
+def fitting_problem(n, seed, dt=1e-5, nchunks=10, ksteps=50, noise=1e-2, solver=2):
     """Targets: trajectories of perturbed true parameters plus Gaussian noise."""
     rng = np.random.default_rng(seed)
     true_p = NOMINAL * rng.uniform(0.5, 1.5, (n, 6))
     y0 = np.tile(Y0, (n, 1))
-    rec = Oracle("oculomotor").run(2, np.zeros(n), y0, true_p, neq=6, npar=6, dt=dt, ksteps=ksteps,
+    rec = Oracle("oculomotor").run(solver, np.zeros(n), y0, true_p, neq=6, npar=6, dt=dt, ksteps=ksteps,
                                    nchunks=nchunks).records
     targets = rec + rng.normal(0, noise, rec.shape)
     guess = true_p * rng.uniform(0.95, 1.05, (n, 6))
@@ -97,6 +97,36 @@ def test_adjoint_matches_reference_gradient(solver, products):
     scale_y = np.abs(gy_r).max(axis=1, keepdims=True)
     assert np.max(np.abs(gp[:8] - gp_r) / scale_p) < 1e-9
     assert np.max(np.abs(gy[:8] - gy_r) / scale_y) < 1e-9
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("products", ["vjp", "jacobians", "tape"])
+@pytest.mark.parametrize("solver", ["ie", "im"])
+def test_implicit_adjoint_matches_reference_gradient(solver, products):
+    """Implicit Euler / midpoint at dt 1e-3: the adjoint of the exact implicit
+    step (transposed solve with the full Jacobian) against dual numbers pushed
+    through the reference's Newton passes.  With the passes run to 1e-12 the
+    two derivatives coincide to the iteration's convergence."""
+    torch = pytest.importorskip("torch")
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.fit import Adjoint
+
+    n, nchunks, ksteps, dt, tol = 48, 5, 20, 1e-3, 1e-12
+    sid = 3 if solver == "ie" else 4
+    t0, y0, p, tg = fitting_problem(n, 5, dt=dt, nchunks=nchunks, ksteps=ksteps, solver=sid)
+    loss_r, gp_r, gy_r = reference_gradient(system_path("oculomotor"), sid, 6, 6, dt, ksteps, nchunks, t0[:8], y0[:8],
+                                            p[:8], tg[:, :, :8], newton_tol=tol, newton_max_iter=200)
+    sim = Integrator(None, solver, dt=dt, tspan=(nchunks * ksteps - 0.5) * dt, ksteps=ksteps, neq=6, npar=6,
+                     orbits=n, newton_tol=tol, newton_max_iter=200, system_src=oculomotor_source(products))
+    T = lambda a: torch.tensor(a, device="cuda")  # noqa: E731
+    loss, gp, gy, flags = Adjoint(sim, use_tape=products == "tape")(T(t0), T(y0), T(p), T(tg))
+    loss, gp, gy, flags = loss.cpu().numpy(), gp.cpu().numpy(), gy.cpu().numpy(), flags.cpu().numpy()
+    assert not flags.any()
+    np.testing.assert_allclose(loss[:8], loss_r, rtol=1e-9)
+    err_p = np.max(np.abs(gp[:8] - gp_r) / np.abs(gp_r).max(axis=1, keepdims=True))
+    err_y = np.max(np.abs(gy[:8] - gy_r) / np.abs(gy_r).max(axis=1, keepdims=True))
+    print("%s/%s adjoint vs dual numbers: params %.2e, y0 %.2e" % (solver, products, err_p, err_y))
+    assert err_p < 1e-7 and err_y < 1e-7
 
 
 @pytest.mark.gpu
