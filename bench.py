@@ -402,24 +402,13 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
                            "calc_jacobian_params; adjoint_tape_ms: reverse mode over sode_system"}
 
 
-def batch_lanes(system, neq):
-    """The batch's automatic lanes per orbit for a class (about two rows per
-    lane from 12 equations up, for files with the per-row functions)."""
-    if system != "kuramoto" or neq < 12:
-        return 1
-    lanes = 4
-    while lanes < 32 and 2 * lanes < neq:
-        lanes *= 2
-    return lanes
-
-
 def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
     """The uneven-sweep shape: orbits mixing Kuramoto N in {4, 16, 64} and the
     oculomotor model, solver per orbit in {Euler, RK4, implicit Euler}, step
     counts log-uniform in [10^2, max_steps], FP64.  The full configuration is
     2^18 orbits and steps up to 10^5; this sample (2^15 orbits, up to 10^4
-    steps) keeps the default run short.  Wide classes run lanes per orbit, in
-    the batch and in the padded launches alike.  One persistent launch from
+    steps) keeps the default run short.  Wide classes run lanes per orbit (the
+    tuner's choice per class), in the batch and in the padded launches alike.  One persistent launch from
     device work queues (autotuned launch shape, graph replay), against the
     padded alternative: one launch per class through the single-system kernel,
     every orbit of a class run for that class's longest step count."""
@@ -463,7 +452,9 @@ def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
         times.append(b.run(graph=True))
     batch_ms = float(np.median(times))
     useful = int(steps.sum())
-    # padded: per class, every orbit runs the class's longest orbit
+    # padded: per class, every orbit runs the class's longest orbit, with the
+    # lanes per orbit the tuner chose for the class
+    tuned_lanes = b.lanes
     padded_ms = 0.0
     stream = torch.cuda.current_stream(dev)
     for k, (system, solver, neq, npar, dt) in enumerate(classes):
@@ -472,7 +463,7 @@ def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
             continue
         m = int(steps[idx].max())
         sim = Integrator(system_path(system), solver, dt=dt, tspan=(m - 0.5) * dt, ksteps=m, neq=neq, npar=npar,
-                         orbits=idx.size, lanes=batch_lanes(system, neq))
+                         orbits=idx.size, lanes=tuned_lanes[k])
         td = torch.zeros(idx.size, dtype=torch.float64, device=dev)
         yd = torch.tensor(np.stack([y0[i] for i in idx]), device=dev)
         pd = torch.tensor(np.stack([p[i] for i in idx]), device=dev)
@@ -487,7 +478,7 @@ def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
             "orbit_steps": useful, "batch_ms": batch_ms, "value": useful / (batch_ms * 1e-3), "unit": METRIC,
             "tuned_launch": {"block": block, "blocks_per_sm": bps}, "padded_per_class_ms": padded_ms,
             "speedup_vs_padded": padded_ms / batch_ms, "registers": b.kernel_info()["registers"],
-            "lanes_per_class": [batch_lanes(c[0], c[2]) for c in classes]}
+            "lanes_per_class": b.lanes}
 
 
 def stochastic_kuramoto_companion(dev, stream, n=1 << 18, N=32, nsteps=2000, ksteps=200, seed=3):

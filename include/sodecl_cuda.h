@@ -298,9 +298,13 @@ int sodecl_batch_set_items(sodecl_batch *b, int64_t n, const int32_t *item_class
  * (32 / lanes) x (slot) bytes of shared memory per warp; a block size whose
  * warps need more than 48 KiB in all is rejected. */
 int sodecl_batch_set_launch(sodecl_batch *b, int32_t block, int32_t blocks_per_sm);
-/* Autotuner: times every candidate launch shape on the current items (each
- * trial advances them) and keeps the fastest. */
+/* Autotuner: times candidate lanes per orbit for the classes whose
+ * lanes_per_orbit is automatic (rebuilding the program for each), then every
+ * candidate launch shape, on the current items (each trial advances them),
+ * and keeps the fastest. */
 int sodecl_batch_tune(sodecl_batch *b, int32_t *block, int32_t *blocks_per_sm, double *best_ms);
+/* Lanes per orbit each class runs with (one entry per class). */
+int sodecl_batch_class_lanes(const sodecl_batch *b, int32_t *lanes);
 /* One persistent launch over every item from its current state; use_graph:
  * replay a captured CUDA graph (captured on first use). */
 int sodecl_batch_run(sodecl_batch *b, int32_t use_graph);

@@ -153,6 +153,7 @@ SIGNATURES = {
     "sodecl_batch_set_items": (C.c_int, [_P, C.c_int64, _P, _P, _P, _P, _P, _P]),
     "sodecl_batch_set_launch": (C.c_int, [_P, C.c_int32, C.c_int32]),
     "sodecl_batch_tune": (C.c_int, [_P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),
+    "sodecl_batch_class_lanes": (C.c_int, [_P, C.POINTER(C.c_int32)]),
     "sodecl_batch_run": (C.c_int, [_P, C.c_int32]),
     "sodecl_batch_results": (C.c_int, [_P, _P, _P, _P, _P, _P]),
     "sodecl_batch_last_ms": (C.c_int, [_P, C.POINTER(C.c_double)]),

@@ -86,9 +86,20 @@ class Batch:
         self._check(N.lib.sodecl_batch_set_launch(self._b, block, blocks_per_sm))
 
     def tune(self):
+        """Times lanes per orbit for the automatic classes, then launch shapes,
+        on the current items (every trial advances them); returns (threads per
+        block, resident blocks per SM, best ms).  `lanes` gives the classes'
+        lanes per orbit."""
         blk, bps, ms = C.c_int32(), C.c_int32(), C.c_double()
         self._check(N.lib.sodecl_batch_tune(self._b, C.byref(blk), C.byref(bps), C.byref(ms)))
         return blk.value, bps.value, ms.value
+
+    @property
+    def lanes(self):
+        """Lanes per orbit of each class."""
+        out = (C.c_int32 * max(1, len(self.classes)))()
+        self._check(N.lib.sodecl_batch_class_lanes(self._b, out))
+        return [int(v) for v in out[:len(self.classes)]]
 
     def run(self, graph=True):
         self._check(N.lib.sodecl_batch_run(self._b, 1 if graph else 0))

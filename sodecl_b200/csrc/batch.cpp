@@ -89,6 +89,43 @@ double step_cost(const sodecl_b200::ProgramSpec &s)
     }
 }
 
+// A warp's slots of a lanes-per-orbit class fit half the 48 KiB cap, so any
+// block of up to 64 threads can launch.
+bool lanes_fit(const sodecl_b200::ProgramSpec &s)
+{
+    return (32 / s.lanes) * sodecl_b200::lanes_slot_words(s) * sizeof(double) * 2 <= sodecl_b200_batch::kSharedCap;
+}
+
+// Rebuilds the program with these lanes per orbit per class (no-op when they
+// are the current ones) and loads it in place of the current one.
+int load_lanes(sodecl_batch *b, const std::vector<int> &lanes)
+{
+    bool same = true;
+    for (size_t k = 0; k < b->classes.size(); ++k) same = same && b->classes[k].def.spec.lanes == lanes[k];
+    if (same && b->prog) return SODECL_OK;
+    for (size_t k = 0; k < b->classes.size(); ++k) b->classes[k].def.spec.lanes = lanes[k];
+    std::vector<sodecl_b200::BatchClass> defs;
+    for (const auto &c : b->classes) defs.push_back(c.def);
+    try {
+        b->prog = sodecl_b200::build_batch(defs, b->fmad != 0, b->division == SODECL_DIV_RECIPROCAL, 256);
+    } catch (const std::exception &ex) {
+        return b->fail(SODECL_ERR_COMPILE, ex.what());
+    }
+    b->warp_words = sodecl_b200::batch_warp_words(defs);
+    drop_graph(b);
+    if (b->lib) {
+        if (b->stream) cudaStreamSynchronize(b->stream);
+        cudaLibraryUnload(b->lib);
+        b->lib = nullptr;
+        b->kernel = nullptr;
+        BATCH_TRY(b, cudaLibraryLoadData(&b->lib, b->prog->cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0));
+        BATCH_TRY(b, cudaLibraryGetKernel(&b->kernel, b->lib, b->prog->kernel_name.c_str()));
+    }
+    while (b->block > 32 && sodecl_b200_batch::shared_bytes(b, b->block) > sodecl_b200_batch::kSharedCap)
+        b->block -= 32;
+    return SODECL_OK;
+}
+
 int grid_size(sodecl_batch *b, int block)
 {
     int per_sm = 0;
@@ -181,15 +218,10 @@ int sodecl_batch_add_class(sodecl_batch *b, const char *system_src, size_t len, 
         return b->fail(SODECL_ERR_UNSUPPORTED, "lanes per orbit need sode_system_row(...) in the system file, and "
                                                "sode_system_stoch_row(...) for the stochastic solver or "
                                                "calc_jacobian_band(...) for the implicit ones");
-    s.lanes = 1;
-    if (c.lanes_per_orbit > 1) {
-        s.lanes = c.lanes_per_orbit;
-    } else if (c.lanes_per_orbit == 0 && rows && c.num_equat >= 12) {
-        // about two rows per lane
-        s.lanes = 4;
-        while (s.lanes < 32 && 2 * s.lanes < c.num_equat) s.lanes *= 2;
-    }
-    if (s.lanes > 1 && (32 / s.lanes) * sodecl_b200::lanes_slot_words(s) * sizeof(double) * 2 > sodecl_b200_batch::kSharedCap)
+    cl.requested_lanes = c.lanes_per_orbit;
+    cl.rows = rows;
+    s.lanes = sodecl_b200_batch::class_lanes(cl, 0);
+    if (s.lanes > 1 && !lanes_fit(s))
         return b->fail(SODECL_ERR_UNSUPPORTED, "lanes per orbit: one warp's orbits need more than half of a block's "
                                                "shared memory");
     cl.cost_per_step = step_cost(s);
@@ -416,12 +448,45 @@ int sodecl_batch_results(sodecl_batch *b, double *t, double *y, double *counters
 
 int sodecl_batch_tune(sodecl_batch *b, int32_t *block, int32_t *blocks_per_sm, double *best_ms)
 {
-    // Times the run for each launch shape and keeps the fastest.  Each trial
-    // integrates the current items from their current state, so callers tune
-    // on a copy of the workload (e.g. shortened step counts) and then upload
-    // the real items.
+    // Times the run for each candidate and keeps the fastest: first the lanes
+    // per orbit of the automatic classes (the heuristic, one lane, twice and
+    // half the heuristic; each a rebuilt program, cached on disk), then the
+    // launch shape.  Each trial integrates the current items from their
+    // current state, so callers tune on a copy of the workload (e.g.
+    // shortened step counts) and then upload the real items.
     if (!b) return SODECL_ERR_INVALID_ARG;
     if (!b->nitems) return b->fail(SODECL_ERR_STATE, "no items to tune on");
+    bool tunable = false;
+    for (const auto &c : b->classes) tunable = tunable || (c.requested_lanes == 0 && c.rows);
+    if (tunable) {
+        std::vector<std::vector<int>> tried;
+        std::vector<int> best_lanes;
+        double best_lanes_ms = 1e300;
+        for (int v = 0; v < 4; ++v) {
+            std::vector<int> lanes;
+            bool fits = true;
+            for (const auto &c : b->classes) {
+                sodecl_b200::ProgramSpec sp = c.def.spec;
+                sp.lanes = sodecl_b200_batch::class_lanes(c, v);
+                fits = fits && (sp.lanes == 1 || lanes_fit(sp));
+                lanes.push_back(sp.lanes);
+            }
+            if (!fits || std::find(tried.begin(), tried.end(), lanes) != tried.end()) continue;
+            tried.push_back(lanes);
+            int rc = load_lanes(b, lanes);
+            if (rc != SODECL_OK) return rc;
+            rc = sodecl_batch_set_launch(b, std::min(b->block, 128), 0);
+            if (rc != SODECL_OK) return rc;
+            rc = sodecl_batch_run(b, 0);
+            if (rc != SODECL_OK) return rc;
+            if (b->last_ms < best_lanes_ms) {
+                best_lanes_ms = b->last_ms;
+                best_lanes = lanes;
+            }
+        }
+        const int rc = load_lanes(b, best_lanes);
+        if (rc != SODECL_OK) return rc;
+    }
     static const int shapes[][2] = {{64, 0}, {128, 0}, {256, 0}, {128, 2}, {256, 1}, {64, 4}};
     double best = 1e300;
     int best_block = b->block, best_bps = b->blocks_per_sm;
@@ -441,6 +506,13 @@ int sodecl_batch_tune(sodecl_batch *b, int32_t *block, int32_t *blocks_per_sm, d
     if (block) *block = best_block;
     if (blocks_per_sm) *blocks_per_sm = best_bps;
     if (best_ms) *best_ms = best;
+    return SODECL_OK;
+}
+
+int sodecl_batch_class_lanes(const sodecl_batch *b, int32_t *lanes)
+{
+    if (!b || !lanes) return SODECL_ERR_INVALID_ARG;
+    for (size_t k = 0; k < b->classes.size(); ++k) lanes[k] = b->classes[k].def.spec.lanes;
     return SODECL_OK;
 }
 

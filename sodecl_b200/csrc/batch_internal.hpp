@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <memory>
 #include <string>
 #include <vector>
@@ -37,7 +38,30 @@ struct BatchArgs {
 struct Class {
     sodecl_b200::BatchClass def;
     double cost_per_step = 1.0;  // relative estimate, orders the classes
+    int requested_lanes = 0;     // sodecl_class_cfg.lanes_per_orbit (0: automatic, tunable)
+    bool rows = false;           // the system file has the per-row functions this solver needs
 };
+
+// Lanes per orbit for an automatic class: about two rows per lane from 12
+// equations up (variant 0); the tuner also tries one lane (1), twice (2) and
+// half (3) that.  Explicit choices are kept.
+inline int class_lanes(const Class &c, int variant)
+{
+    if (c.requested_lanes > 0) return c.requested_lanes;
+    if (!c.rows) return 1;
+    const int neq = c.def.spec.num_equat;
+    int lanes = 1;
+    if (neq >= 12) {
+        lanes = 4;
+        while (lanes < 32 && 2 * lanes < neq) lanes *= 2;
+    }
+    switch (variant) {
+    case 1: return 1;
+    case 2: return neq >= 4 ? std::min(32, lanes * 2 > 1 ? lanes * 2 : 4) : lanes;
+    case 3: return lanes >= 4 ? lanes / 2 : lanes;
+    default: return lanes;
+    }
+}
 
 }  // namespace sodecl_b200_batch
 

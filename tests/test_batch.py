@@ -163,6 +163,39 @@ def test_batch_tuner_and_launch_shapes_agree():
     assert block in (64, 128, 256) and ms > 0
 
 
+@pytest.mark.gpu
+def test_batch_tuner_picks_lanes_and_keeps_results():
+    """The tuner times lanes per orbit for automatic classes (program rebuilt
+    per candidate); whatever it picks, the states equal the untuned run's bit
+    for bit without FMA contraction."""
+    classes = [c[:6] for c in LANES_CLASSES]
+    n = 600
+    cls, nsteps, t0, y0, p, counters = make_items(n, 8, classes=classes, steps=(0, 1, 7, 50))
+
+    def build():
+        b = Batch(fmad=False)
+        for system, solver, neq, npar, nnoi, dt, lanes in LANES_CLASSES:
+            b.add_class(system_path(system), solver, neq=neq, npar=npar, nnoi=nnoi, dt=dt, lanes=lanes)
+        return b.compile()
+
+    want = build()
+    want.set_items(cls, nsteps, t0, y0, p, counters)
+    want.run()
+    tuned = build()
+    tuned.set_items(cls, nsteps, t0, y0, p, counters)
+    tuned.tune()
+    lanes = tuned.lanes
+    print("tuned lanes per class:", lanes)
+    assert lanes[0] == 32 and lanes[2] == 4  # explicit choices are kept
+    tuned.set_items(cls, nsteps, t0, y0, p, counters)
+    tuned.run()
+    for a, b in zip(want.results(), tuned.results()):
+        if isinstance(a, list):
+            np.testing.assert_array_equal(np.concatenate(a), np.concatenate(b))
+        else:
+            np.testing.assert_array_equal(a, b)
+
+
 # (system, solver, neq, npar, nnoi, dt, lanes): wide classes with lanes per orbit
 # (0: automatic), next to one-lane classes in the same program
 LANES_CLASSES = [("kuramoto", "ie", 64, 65, 0, 0.01, 32), ("kuramoto", "se", 32, 65, 32, 0.01, 0),
