@@ -308,6 +308,7 @@ def main():
         extras["gradient"] = gradient_companion(dev)
         extras["uneven_batch"] = batch_companion(dev)
         extras["stochastic_kuramoto"] = stochastic_kuramoto_companion(dev, stream)
+        extras["small_kuramoto"] = small_kuramoto_companion(dev, stream)
 
     cpu = None
     if rank == 0 and world == 1:
@@ -408,33 +409,19 @@ def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
     counts log-uniform in [10^2, max_steps], FP64.  The full configuration is
     2^18 orbits and steps up to 10^5; this sample (2^15 orbits, up to 10^4
     steps) keeps the default run short.  Wide classes run lanes per orbit (the
-    tuner's choice per class), in the batch and in the padded launches alike.  One persistent launch from
-    device work queues (autotuned launch shape, graph replay), against the
-    padded alternative: one launch per class through the single-system kernel,
-    every orbit of a class run for that class's longest step count."""
+    tuner's choice per class), in the batch and in the padded launches alike.
+    One persistent launch from device work queues (autotuned launch shape,
+    graph replay), against the padded alternative: one launch per class
+    through the single-system kernel, every orbit of a class run for that
+    class's longest step count."""
     import torch
 
     from sodecl_b200 import Integrator, system_path
     from sodecl_b200.batch import Batch
 
-    rng = np.random.default_rng(seed)
-    classes = []
-    for N in (4, 16, 64):
-        for solver in ("euler", "rk4", "ie"):
-            classes.append(("kuramoto", solver, N, N + 1, 0.01))
-    for solver, dt in (("euler", 1e-6), ("rk4", 1e-5), ("ie", 1e-3)):
-        classes.append(("oculomotor", solver, 6, 6, dt))
-    cls = rng.integers(0, len(classes), n).astype(np.int32)
-    steps = np.exp(rng.uniform(np.log(100), np.log(max_steps), n)).astype(np.int64)
-    y0, p = [], []
-    for c in cls:
-        system, solver, neq, npar, dt = classes[c]
-        if system == "oculomotor":
-            y0.append(Y0)
-            p.append(NOMINAL * rng.uniform(0.5, 1.5, 6))
-        else:
-            y0.append(rng.uniform(0, 2 * np.pi, neq))
-            p.append(np.concatenate([[rng.uniform(0, 5)], rng.normal(size=neq)]))
+    from sodecl_b200.workloads import uneven_batch
+
+    classes, cls, steps, y0, p, rng = uneven_batch(n, max_steps, seed)
     b = Batch()
     for system, solver, neq, npar, dt in classes:
         b.add_class(system_path(system), solver, neq=neq, npar=npar, dt=dt)
@@ -532,32 +519,41 @@ def stochastic_kuramoto_companion(dev, stream, n=1 << 18, N=32, nsteps=2000, kst
 
 def companions(a, n, dev, stream):
     """Same shape, other settings: the stable step dt=1e-5 (RK4 diverges at
-    1e-3 for most parameter draws), FP32, and implicit midpoint."""
+    1e-3 for most parameter draws), FP32, and implicit midpoint -- with the
+    reference's Newton settings (1e-7, up to 1000 passes) and with the stated
+    1e-10 / 10 passes, which the reference's banded solve does not converge
+    within (the orbits that hit the limit are counted)."""
     import torch
 
     from sodecl_b200 import Integrator, system_path
 
     out = {}
     t0, y0, p = workload(n, 0)
-    cases = [("stable_dt_1e-5", a.solver, 1e-5, a.precision), ("fp32", a.solver, a.dt, "fp32"),
-             ("fp32_stable_dt_1e-5", a.solver, 1e-5, "fp32"), ("implicit_midpoint", "im", a.dt, "fp64")]
-    for name, solver, dt, prec in cases:
+    # (name, solver, dt, precision, Newton tolerance, Newton pass limit)
+    cases = [("stable_dt_1e-5", a.solver, 1e-5, a.precision, 1e-7, 1000), ("fp32", a.solver, a.dt, "fp32", 1e-7, 1000),
+             ("fp32_stable_dt_1e-5", a.solver, 1e-5, "fp32", 1e-7, 1000),
+             ("implicit_midpoint", "im", a.dt, "fp64", 1e-7, 1000),
+             ("implicit_midpoint_tol1e-10_max10", "im", a.dt, "fp64", 1e-10, 10),
+             ("implicit_midpoint_fp32_tol1e-10_max10", "im", a.dt, "fp32", 1e-10, 10)]
+    for name, solver, dt, prec, tol, maxit in cases:
         sim = Integrator(system_path("oculomotor"), solver, dt=dt, tspan=a.nsteps * dt, ksteps=a.ksteps, neq=6,
-                         npar=6, orbits=n, precision=prec)
+                         npar=6, orbits=n, precision=prec, newton_tol=tol, newton_max_iter=maxit)
         nrec = sim.num_records
         td, yd, pd = torch.tensor(t0, device=dev), torch.tensor(y0, device=dev), torch.tensor(p, device=dev)
         rec = torch.empty((nrec, 6, n), dtype=torch.float64, device=dev)
         passes = torch.zeros(n, dtype=torch.int64, device=dev)
+        flags = torch.zeros(n, dtype=torch.int32, device=dev)
         ms = []
         for it in range(3):
             td.copy_(torch.tensor(t0, device=dev))
             yd.copy_(torch.tensor(y0, device=dev))
             passes.zero_()
+            flags.zero_()
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record(stream)
             sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(), records=rec.data_ptr(), n=n,
                        chunk_begin=0, chunk_end=sim.num_chunks, newton_passes=passes.data_ptr(),
-                       stream=stream.cuda_stream)
+                       flags=flags.data_ptr(), stream=stream.cuda_stream)
             e.record(stream)
             torch.cuda.synchronize()
             if it > 0:
@@ -568,11 +564,47 @@ def companions(a, n, dev, stream):
                  "nan_fraction_final": float(np.mean(~np.isfinite(last).all(axis=0)))}
         if solver == "im":
             entry["newton_passes_per_step"] = float(passes.double().mean().item() / a.nsteps)
+            entry["newton"] = {"tol": tol, "max_passes": maxit,
+                               "orbits_at_pass_limit": float((flags & 1).bool().double().mean().item())}
         out[name] = entry
         sim.close()
         del rec
         torch.cuda.empty_cache()
     return {"companions": out}
+
+
+def small_kuramoto_companion(dev, stream):
+    """The plain CPU-sized case: Kuramoto N=8, 1024 orbits, K ~ U(0,5) per orbit,
+    omega ~ N(0,1) shared, theta0 ~ U(0, 2 pi), explicit Euler, dt 0.05, 1000
+    steps, a record every 10 (101 records), FP64.  One launch; at this size it
+    is latency-bound (1024 threads on 148 SMs)."""
+    import torch
+
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.workloads import kuramoto
+
+    n, N, nsteps, ksteps, dt = 1024, 8, 1000, 10, 0.05
+    t0, th0, p, _ = kuramoto(n, N, seed=11)
+    sim = Integrator(system_path("kuramoto"), "euler", dt=dt, tspan=nsteps * dt, ksteps=ksteps, neq=N, npar=N + 1,
+                     orbits=n)
+    T = lambda x: torch.tensor(x, device=dev)  # noqa: E731
+    td, yd, pd = T(t0), T(th0), T(p)
+    rec = torch.empty((sim.num_records, N, n), dtype=torch.float64, device=dev)
+    ms = []
+    for it in range(4):
+        td.copy_(T(t0))
+        yd.copy_(T(th0))
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(), records=rec.data_ptr(),
+                   stream=stream.cuda_stream)
+        e.record(stream)
+        torch.cuda.synchronize()
+        if it > 0:
+            ms.append(s.elapsed_time(e))
+    sim.close()
+    return {"orbits": n, "N": N, "nsteps": nsteps, "records": nsteps // ksteps + 1, "ms": float(np.mean(ms)),
+            "value": n * nsteps / (np.mean(ms) * 1e-3), "unit": METRIC}
 
 
 if __name__ == "__main__":

@@ -12,6 +12,9 @@ Shapes (all inputs seeded; no dataset is involved):
                         orbit, counters orbit * 2^20; dt 0.01, a record every 200
   kuramoto-<solver>     deterministic Kuramoto: N phases, K ~ U(0,5), omega ~ N(0,1)
                         shared, theta0 ~ U(0, 2 pi); dt 0.01
+  uneven-batch          the persistent batch kernel over the uneven sweep: Kuramoto
+                        N in {4, 16, 64} and the oculomotor model x {Euler, RK4,
+                        implicit Euler}, step counts log-uniform in [100, max-steps]
   adjoint-oculomotor    loss and gradient (sodecl_cuda_adjoint) of the oculomotor
                         RK4 fit: targets from seeded true parameters + N(0, 1e-2)
                         noise, gradient at parameters within +-5 % of them; dt 1e-5
@@ -45,6 +48,53 @@ def kuramoto(n, N, seed=3, noise=False):
     theta0 = rng.uniform(0, 2 * np.pi, (n, N))
     counters = np.arange(n) * 2.0 ** 20 if noise else None
     return np.zeros(n), theta0, params, counters
+
+
+# the uneven sweep's classes: (system, solver, equations, parameters, dt)
+UNEVEN_CLASSES = [("kuramoto", solver, N, N + 1, 0.01) for N in (4, 16, 64) for solver in ("euler", "rk4", "ie")] + \
+                 [("oculomotor", solver, 6, 6, dt) for solver, dt in (("euler", 1e-6), ("rk4", 1e-5), ("ie", 1e-3))]
+
+
+def uneven_batch(n, max_steps, seed=4):
+    """(classes, class per orbit, step counts, y0 list, params list, generator)
+    of the uneven sweep: Kuramoto N in {4, 16, 64} and the oculomotor model,
+    solver in {Euler, RK4, implicit Euler} (12 classes, drawn uniformly), step
+    counts log-uniform in [10^2, max_steps]."""
+    rng = np.random.default_rng(seed)
+    cls = rng.integers(0, len(UNEVEN_CLASSES), n).astype(np.int32)
+    steps = np.exp(rng.uniform(np.log(100), np.log(max_steps), n)).astype(np.int64)
+    y0, p = [], []
+    for c in cls:
+        system, solver, neq, npar, dt = UNEVEN_CLASSES[c]
+        if system == "oculomotor":
+            y0.append(Y0)
+            p.append(NOMINAL * rng.uniform(0.5, 1.5, 6))
+        else:
+            y0.append(rng.uniform(0, 2 * np.pi, neq))
+            p.append(np.concatenate([[rng.uniform(0, 5)], rng.normal(size=neq)]))
+    return UNEVEN_CLASSES, cls, steps, y0, p, rng
+
+
+def _batch_main(a):
+    from . import system_path
+    from .batch import Batch
+
+    classes, cls, steps, y0, p, rng = uneven_batch(a.orbits, a.max_steps)
+    b = Batch()
+    for system, solver, neq, npar, dt in classes:
+        b.add_class(system_path(system), solver, neq=neq, npar=npar, dt=dt)
+    b.compile()
+    # tune on a shortened copy of an eighth of the orbits (trials advance them)
+    sample = rng.choice(a.orbits, max(1, a.orbits // 8), replace=False)
+    b.set_items(cls[sample], np.minimum(steps[sample], 200), np.zeros(sample.size), [y0[i] for i in sample],
+                [p[i] for i in sample])
+    block, bps, _ = b.tune()
+    for k in range(a.launches):
+        b.set_items(cls, steps, np.zeros(a.orbits), y0, p)
+        ms = b.run(graph=True)
+        print(json.dumps({"case": a.case, "launch": k, "ms": ms, "orbits": a.orbits, "max_steps": a.max_steps,
+                          "orbit_steps": int(steps.sum()), "orbit_steps_per_s": int(steps.sum()) / (ms * 1e-3),
+                          "block": block, "blocks_per_sm": bps, "lanes": b.lanes}), flush=True)
 
 
 def fitting_targets(n, nsteps, ksteps, dt, seed=55, device="cuda"):
@@ -95,7 +145,8 @@ def _adjoint_main(a):
 
 def _parse():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("case", help="oculomotor-<solver> | stochastic-kuramoto | kuramoto-<solver>")
+    ap.add_argument("case", help="oculomotor-<solver> | stochastic-kuramoto | kuramoto-<solver> | uneven-batch | "
+                                 "adjoint-oculomotor")
     ap.add_argument("--orbits", type=int, default=1 << 15)
     ap.add_argument("--nsteps", type=int, default=200)
     ap.add_argument("--ksteps", type=int, default=100)
@@ -107,6 +158,7 @@ def _parse():
     ap.add_argument("--division", default="ieee", choices=["ieee", "reciprocal"])
     ap.add_argument("--min-blocks", type=int, default=0)
     ap.add_argument("--launches", type=int, default=2)
+    ap.add_argument("--max-steps", type=int, default=10000, help="uneven-batch: longest step count")
     return ap.parse_args()
 
 
@@ -119,6 +171,8 @@ def main():
     n = a.orbits
     if a.case == "adjoint-oculomotor":
         return _adjoint_main(a)
+    if a.case == "uneven-batch":
+        return _batch_main(a)
     if a.case.startswith("oculomotor"):
         solver = a.case.split("-", 1)[1] if "-" in a.case else "rk4"
         dt = a.dt if a.dt is not None else 1e-3
