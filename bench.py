@@ -577,7 +577,8 @@ def small_kuramoto_companion(dev, stream):
     """The plain CPU-sized case: Kuramoto N=8, 1024 orbits, K ~ U(0,5) per orbit,
     omega ~ N(0,1) shared, theta0 ~ U(0, 2 pi), explicit Euler, dt 0.05, 1000
     steps, a record every 10 (101 records), FP64.  One launch; at this size it
-    is latency-bound (1024 threads on 148 SMs)."""
+    is latency-bound (1024 orbits on 148 SMs), so the tuner's lanes per orbit
+    (several lanes sharing one orbit's 8 rows) shorten each orbit's steps."""
     import torch
 
     from sodecl_b200 import Integrator, system_path
@@ -585,26 +586,33 @@ def small_kuramoto_companion(dev, stream):
 
     n, N, nsteps, ksteps, dt = 1024, 8, 1000, 10, 0.05
     t0, th0, p, _ = kuramoto(n, N, seed=11)
-    sim = Integrator(system_path("kuramoto"), "euler", dt=dt, tspan=nsteps * dt, ksteps=ksteps, neq=N, npar=N + 1,
-                     orbits=n)
+    out = {"orbits": n, "N": N, "nsteps": nsteps, "records": nsteps // ksteps + 1, "unit": METRIC}
     T = lambda x: torch.tensor(x, device=dev)  # noqa: E731
-    td, yd, pd = T(t0), T(th0), T(p)
-    rec = torch.empty((sim.num_records, N, n), dtype=torch.float64, device=dev)
-    ms = []
-    for it in range(4):
-        td.copy_(T(t0))
-        yd.copy_(T(th0))
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record(stream)
-        sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(), records=rec.data_ptr(),
-                   stream=stream.cuda_stream)
-        e.record(stream)
-        torch.cuda.synchronize()
-        if it > 0:
-            ms.append(s.elapsed_time(e))
-    sim.close()
-    return {"orbits": n, "N": N, "nsteps": nsteps, "records": nsteps // ksteps + 1, "ms": float(np.mean(ms)),
-            "value": n * nsteps / (np.mean(ms) * 1e-3), "unit": METRIC}
+    for name, tune in (("one_thread_per_orbit", False), ("tuned", True)):
+        sim = Integrator(system_path("kuramoto"), "euler", dt=dt, tspan=nsteps * dt, ksteps=ksteps, neq=N,
+                         npar=N + 1, orbits=n)
+        choice = None
+        if tune:
+            sim.upload(t0, th0, p)
+            choice = sim.autotune(sample_orbits=n, sample_steps=200)
+        td, yd, pd = T(t0), T(th0), T(p)
+        rec = torch.empty((sim.num_records, N, n), dtype=torch.float64, device=dev)
+        ms = []
+        for it in range(4):
+            td.copy_(T(t0))
+            yd.copy_(T(th0))
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(), records=rec.data_ptr(),
+                       stream=stream.cuda_stream)
+            e.record(stream)
+            torch.cuda.synchronize()
+            if it > 0:
+                ms.append(s.elapsed_time(e))
+        sim.close()
+        out[name] = {"ms": float(np.mean(ms)), "value": n * nsteps / (np.mean(ms) * 1e-3),
+                     "launch": choice or {"lanes": 1, "block": 128}}
+    return out
 
 
 if __name__ == "__main__":

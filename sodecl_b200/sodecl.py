@@ -11,6 +11,11 @@ results has shape (orbits*nequat, records); row eq*orbits + orbit.  The
 platform argument is ignored and the device is the CUDA ordinal.  Extra
 keywords (precision, fmad, newton_tol, newton_max_iter, counters) expose this
 library's options.
+
+t is built as the reference builds it, numpy.arange(0, tspan + dt*ksteps,
+dt*ksteps), which in floating point can hold one entry more or fewer than there
+are records (tspan 0.2 with dt*ksteps 0.1: four times, three records).  With
+exact_time=True, t holds one time per record instead: record r at r*dt*ksteps.
 """
 from __future__ import annotations
 
@@ -21,7 +26,7 @@ from . import sodecl_interface
 
 def sodecl(openclplatform, opencldevice, openclkernel, initx, params, sodesolver, orbits, nequat, nnoiseprocesses,
            dt, tspan, ksteps, localgroupsize, *, precision=0, fmad=1, newton_tol=1e-7, newton_max_iter=1000,
-           counters=None):
+           counters=None, exact_time=False):
     # t0 = 0 for every orbit; nparams from the first parameter row (sodecl.py:40-46)
     t0 = numpy.zeros(orbits)
     nparams = numpy.asarray(params)[0].size
@@ -46,9 +51,13 @@ def sodecl(openclplatform, opencldevice, openclkernel, initx, params, sodesolver
 
     results = numpy.asarray(results)
     if results.size == 0:
-        return numpy.arange(0, tspan + dt * ksteps, dt * ksteps), results.reshape(orbits * nequat, 0)
+        t = numpy.zeros(0) if exact_time else numpy.arange(0, tspan + dt * ksteps, dt * ksteps)
+        return t, results.reshape(orbits * nequat, 0)
     results = results.reshape(orbits * nequat, int(results.shape[0] / (orbits * nequat)), order='F')
 
-    # time axis as the reference builds it (sodecl.py:82)
-    t = numpy.arange(0, tspan + dt * ksteps, dt * ksteps)
+    if exact_time:
+        t = numpy.arange(results.shape[1]) * (dt * ksteps)
+    else:
+        # time axis as the reference builds it (sodecl.py:82)
+        t = numpy.arange(0, tspan + dt * ksteps, dt * ksteps)
     return t, results

@@ -103,6 +103,24 @@ def test_reference_known_answers_through_sodecl_py(name, solver, dt, ksteps):
     assert_parity("golden %s" % name, got, want, alt)
 
 
+def test_sodecl_py_time_axis():
+    """The reference's time axis (kept by default) can disagree with the record
+    count; exact_time gives one time per record."""
+    from sodecl_b200.sodecl import sodecl
+
+    orbits = 2
+    initx = np.tile(Y0, (orbits, 1))
+    params = np.tile(NOMINAL, (orbits, 1))
+    # tspan 0.2 with dt*ksteps 0.1: the reference loop makes 2 intervals (3 records)
+    t_ref, res = sodecl(0, 0, system_path("oculomotor"), initx, params, 2, orbits, 6, 0, 1e-3, 0.2, 100, 0)
+    t_exact, res2 = sodecl(0, 0, system_path("oculomotor"), initx, params, 2, orbits, 6, 0, 1e-3, 0.2, 100, 0,
+                           exact_time=True)
+    assert res.shape == (orbits * 6, 3)
+    assert t_ref.size == 4  # as the reference returns it
+    np.testing.assert_allclose(t_exact, [0.0, 0.1, 0.2])
+    np.testing.assert_array_equal(res, res2)
+
+
 def test_reference_python_module_list_interface():
     from sodecl_b200 import sodecl_interface
 
