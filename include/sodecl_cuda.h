@@ -253,6 +253,9 @@ int sodecl_cuda_kernel_info(sodecl_ctx *ctx, int *regs, int *local_bytes, int *m
 int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_steps, int32_t *block,
                          int32_t *min_blocks, int32_t *division, int32_t *lanes, double *best_ms);
 
+/* The context's configuration as it stands, e.g. after sodecl_cuda_autotune. */
+int sodecl_cuda_get_cfg(const sodecl_ctx *ctx, sodecl_cfg *cfg);
+
 /* Division mode the program was actually built with (SODECL_DIV_*): the
  * reciprocal mode falls back to IEEE for system files that need plain double. */
 int sodecl_cuda_program_division(const sodecl_ctx *ctx);

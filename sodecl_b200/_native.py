@@ -138,6 +138,7 @@ SIGNATURES = {
     "sodecl_cuda_device_count": (C.c_int, [C.POINTER(C.c_int)]),
     "sodecl_cuda_launch": (C.c_int, [C.c_void_p, C.POINTER(Launch), C.c_void_p]),
     "sodecl_cuda_program_division": (C.c_int, [C.c_void_p]),
+    "sodecl_cuda_get_cfg": (C.c_int, [C.c_void_p, C.POINTER(Cfg)]),
     "sodecl_cuda_adjoint": (C.c_int, [C.c_void_p, C.POINTER(AdjointIO), C.c_void_p]),
     "sodecl_cuda_autotune": (C.c_int, [C.c_void_p, C.c_int64, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                        C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_double)]),

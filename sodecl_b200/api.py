@@ -124,8 +124,7 @@ class Integrator:
         b, m, d, ln, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
         N.check(N.lib.sodecl_cuda_autotune(self._ctx, int(sample_orbits), int(sample_steps), C.byref(b), C.byref(m),
                                            C.byref(d), C.byref(ln), C.byref(ms)), self._ctx)
-        self.cfg.local_group_size, self.cfg.min_blocks_per_sm, self.cfg.division = b.value, m.value, d.value
-        self.cfg.lanes_per_orbit = ln.value
+        N.check(N.lib.sodecl_cuda_get_cfg(self._ctx, C.byref(self.cfg)), self._ctx)
         return {"block": b.value, "min_blocks": m.value,
                 "division": "reciprocal" if d.value == N.DIV_RECIPROCAL else "ieee", "lanes": ln.value,
                 "sample_ms": ms.value}

@@ -913,6 +913,13 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     return SODECL_OK;
 }
 
+int sodecl_cuda_get_cfg(const sodecl_ctx *ctx, sodecl_cfg *cfg)
+{
+    if (!ctx || !cfg) return SODECL_ERR_INVALID_ARG;
+    *cfg = ctx->cfg;
+    return SODECL_OK;
+}
+
 size_t sodecl_cuda_last_error(const sodecl_ctx *ctx, char *buf, size_t n)
 {
     return copy_string(ctx ? ctx->error : std::string("null context"), buf, n);

@@ -212,3 +212,17 @@ def test_division_modes_and_fallback():
     assert "#define SODECL_FAST_DIV 0" in sim.program_source
     text = Integrator(system_path("oculomotor"), "rk4", division="reciprocal", **kw).program_source
     assert "#define SODECL_FAST_DIV 1" in text and "#define double sodecl_f64" in text
+
+
+def test_get_cfg_returns_the_configuration():
+    cfg = N.Cfg()
+    N.lib.sodecl_cfg_init(C.byref(cfg))
+    cfg.solver, cfg.dt, cfg.int_time, cfg.kernel_steps = N.RUNGE_KUTTA, 1e-5, 1e-4, 10
+    cfg.num_equat, cfg.num_params, cfg.list_size, cfg.local_group_size = 6, 6, 16, 96
+    ctx = C.c_void_p()
+    assert N.lib.sodecl_cuda_create(C.byref(cfg), C.byref(ctx)) == N.OK
+    back = N.Cfg()
+    assert N.lib.sodecl_cuda_get_cfg(ctx, C.byref(back)) == N.OK
+    assert bytes(back) == bytes(cfg)
+    assert N.lib.sodecl_cuda_get_cfg(None, C.byref(back)) == N.ERR_INVALID_ARG
+    N.lib.sodecl_cuda_destroy(ctx)
