@@ -308,10 +308,11 @@ __device__ __forceinline__ void sodecl_transposed_solve(const real_t (*J)[_numeq
 // sodecl_step_euler / sodecl_step_rk4's arithmetic, and of the implicit steps
 // taken as solved exactly.
 __device__ __forceinline__ void sodecl_step_adjoint(double h, double t, const double *y, const double *ynext,
-                                                    const double *p, double *lambda, double *pbar, sodecl_tape *tape,
-                                                    double *adj, int &overflow)
+                                                    const double *stages, const double *p, double *lambda,
+                                                    double *pbar, sodecl_tape *tape, double *adj, int &overflow)
 {
     (void)ynext;
+    (void)stages;
 #if SODECL_SOLVER == 1
     // y1 = y + h f(t, y)
     double seed[_numeq_], ybar[_numeq_];
@@ -323,22 +324,11 @@ __device__ __forceinline__ void sodecl_step_adjoint(double h, double t, const do
     for (int e = 0; e < _numeq_; ++e) lambda[e] = ybar[e];
 #elif SODECL_SOLVER == 2
     // y1 = y + (k1 + 2 k2 + 2 k3 + k4) h / 6 with stage inputs
-    // x1 = y, x2 = y + (h/2) k1, x3 = y + (h/2) k2, x4 = y + h k3
-    double k[_numeq_], x2[_numeq_], x3[_numeq_], x4[_numeq_];
+    // x1 = y, x2 = y + (h/2) k1, x3 = y + (h/2) k2, x4 = y + h k3, recorded
+    // by the segment's recomputation (stages = x2 | x3 | x4)
+    const double *x2 = stages, *x3 = stages + _numeq_, *x4 = stages + 2 * _numeq_;
     double pv[SODECL_NPAR_ALLOC];
     for (int j = 0; j < _numpar_; ++j) pv[j] = p[j];
-    {
-        real_t yy[_numeq_], kk[_numeq_], pp[SODECL_NPAR_ALLOC], xx[_numeq_];
-        for (int e = 0; e < _numeq_; ++e) yy[e] = (real_t)y[e];
-        for (int j = 0; j < _numpar_; ++j) pp[j] = (real_t)pv[j];
-        sode_system((real_t)t, yy, kk, pp);
-        for (int e = 0; e < _numeq_; ++e) { k[e] = (double)kk[e]; xx[e] = yy[e] + ((real_t)h * (real_t)0.50) * kk[e]; x2[e] = (double)xx[e]; }
-        sode_system((real_t)t + (real_t)0.50 * (real_t)h, xx, kk, pp);
-        for (int e = 0; e < _numeq_; ++e) { xx[e] = yy[e] + ((real_t)h * (real_t)0.50) * kk[e]; x3[e] = (double)xx[e]; }
-        sode_system((real_t)t + (real_t)0.50 * (real_t)h, xx, kk, pp);
-        for (int e = 0; e < _numeq_; ++e) { xx[e] = yy[e] + (real_t)h * kk[e]; x4[e] = (double)xx[e]; }
-        (void)k;
-    }
     double ybar[_numeq_], kbar[_numeq_], seed[_numeq_], xbar[_numeq_];
     const double w1 = h / 6.0, w2 = 2.0 * h / 6.0;
     for (int e = 0; e < _numeq_; ++e) ybar[e] = lambda[e];
@@ -412,6 +402,14 @@ __device__ __forceinline__ void sodecl_step_adjoint(double h, double t, const do
 
 #define SODECL_FLAG_TAPE_OVERFLOW 4
 
+// doubles per orbit per segment step: the state, t, and for RK4 the three
+// stage inputs (recorded by the recomputation, read by the reverse step)
+#if SODECL_SOLVER == 2
+#define SODECL_SEG_WIDTH (4 * _numeq_ + 1)
+#else
+#define SODECL_SEG_WIDTH (_numeq_ + 1)
+#endif
+
 struct sodecl_adjoint_args {
     const double *t0;         // [n]
     const double *y0;         // [n][neq]
@@ -422,8 +420,7 @@ struct sodecl_adjoint_args {
     double *grad_y0;          // [n][neq] or null
     double *ckpt;             // scratch [nckpt][neq][n]
     double *ckpt_t;           // scratch [nckpt][n]
-    double *seg;              // scratch [ckpt_every][neq][n]
-    double *seg_t;            // scratch [ckpt_every][n]
+    double *seg;              // scratch [ckpt_every][SODECL_SEG_WIDTH][n]: state, t, (RK4) stage inputs
     int *flags;               // [n] or null
     long long n;
     int nchunks;              // records - 1; steps = nchunks * _numsteps_
@@ -494,10 +491,23 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
         real_t ts = (real_t)a.ckpt_t[(long long)sg * n + i];
         for (int e = 0; e < _numeq_; ++e) ys[e] = (real_t)a.ckpt[((long long)sg * _numeq_ + e) * n + i];
         for (int s = s0; s < s1; ++s) {
-            const long long c = s - s0;
-            a.seg_t[c * n + i] = (double)ts;
-            for (int e = 0; e < _numeq_; ++e) a.seg[(c * _numeq_ + e) * n + i] = (double)ys[e];
+            double *st = a.seg + (long long)(s - s0) * SODECL_SEG_WIDTH * n + i;
+            st[_numeq_ * n] = (double)ts;
+            for (int e = 0; e < _numeq_; ++e) st[e * n] = (double)ys[e];
+#if SODECL_SOLVER == 2
+            // the step with its stage inputs recorded (sodecl_advance's RK4 step)
+            real_t x2[_numeq_], x3[_numeq_], x4[_numeq_], ynew[_numeq_];
+            sodecl_step_rk4(_m_dt_, ts, ys, ynew, p, x2, x3, x4);
+            ts = ts + _m_dt_;
+            for (int e = 0; e < _numeq_; ++e) {
+                ys[e] = ynew[e];
+                st[(_numeq_ + 1 + e) * n] = (double)x2[e];
+                st[(2 * _numeq_ + 1 + e) * n] = (double)x3[e];
+                st[(3 * _numeq_ + 1 + e) * n] = (double)x4[e];
+            }
+#else
             sodecl_advance(ts, ys, p, i, counter, passes, capped);
+#endif
         }
         // reverse the segment's steps
         for (int s = s1 - 1; s >= s0; --s) {
@@ -507,10 +517,11 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
                 for (int e = 0; e < _numeq_; ++e)
                     lambda[e] += 2.0 * w * (ynext[e] - a.targets[((long long)r * _numeq_ + e) * n + i]);
             }
-            const long long c = s - s0;
-            double ystep[_numeq_];
-            for (int e = 0; e < _numeq_; ++e) ystep[e] = a.seg[(c * _numeq_ + e) * n + i];
-            sodecl_step_adjoint((double)_m_dt_, a.seg_t[c * n + i], ystep, ynext, pd, lambda, pbar, tape, adj,
+            const double *st = a.seg + (long long)(s - s0) * SODECL_SEG_WIDTH * n + i;
+            double ystep[_numeq_], stages[SODECL_SEG_WIDTH - _numeq_ - 1 > 0 ? SODECL_SEG_WIDTH - _numeq_ - 1 : 1];
+            for (int e = 0; e < _numeq_; ++e) ystep[e] = st[e * n];
+            for (int e = 0; e < SODECL_SEG_WIDTH - _numeq_ - 1; ++e) stages[e] = st[(_numeq_ + 1 + e) * n];
+            sodecl_step_adjoint((double)_m_dt_, st[_numeq_ * n], ystep, ynext, stages, pd, lambda, pbar, tape, adj,
                                 overflow);
             for (int e = 0; e < _numeq_; ++e) ynext[e] = ystep[e];
         }

@@ -96,8 +96,10 @@ __device__ __forceinline__ void sodecl_step_euler(real_t h, real_t t, real_t *y,
 
 // RK4 with the reference's buffer reuse and accumulation order: the k1 slot
 // accumulates k1 + 2 k2 + 2 k3 in place; result y + (acc + k4) h / 6.
-//                                                   (src/kernels/rk4.cl:17-64)
-__device__ __forceinline__ void sodecl_step_rk4(real_t h, real_t t, real_t *y, real_t *ynew, real_t *p)
+// x2, x3, x4 (optional) receive the stage inputs y + (h/2) k1, y + (h/2) k2,
+// y + h k3 (the adjoint reuses them).             (src/kernels/rk4.cl:17-64)
+__device__ __forceinline__ void sodecl_step_rk4(real_t h, real_t t, real_t *y, real_t *ynew, real_t *p,
+                                                real_t *x2 = nullptr, real_t *x3 = nullptr, real_t *x4 = nullptr)
 {
     real_t stage[_numeq_], probe[_numeq_];
     sode_system(t, y, ynew, p);
@@ -105,18 +107,21 @@ __device__ __forceinline__ void sodecl_step_rk4(real_t h, real_t t, real_t *y, r
     for (int e = 0; e < _numeq_; ++e) {
         stage[e] = ynew[e];
         probe[e] = y[e] + (h * (real_t)0.50) * stage[e];
+        if (x2) x2[e] = probe[e];
     }
     sode_system(t + (real_t)0.50 * h, probe, stage, p);
 #pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) {
         ynew[e] = ynew[e] + (real_t)2.00 * stage[e];
         probe[e] = y[e] + (h * (real_t)0.50) * stage[e];
+        if (x3) x3[e] = probe[e];
     }
     sode_system(t + (real_t)0.50 * h, probe, stage, p);
 #pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) {
         ynew[e] = ynew[e] + (real_t)2.00 * stage[e];
         probe[e] = y[e] + h * stage[e];
+        if (x4) x4[e] = probe[e];
     }
     sode_system(t + h, probe, stage, p);
 #pragma unroll SODECL_EQ_UNROLL

@@ -60,7 +60,6 @@ struct AdjointArgs {
     double *ckpt;
     double *ckpt_t;
     double *seg;
-    double *seg_t;
     int *flags;
     long long n;
     int nchunks;
@@ -874,8 +873,11 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     if (steps > 0 && C > steps) C = static_cast<int>(steps);
     const int64_t nckpt = steps > 0 ? (steps + C - 1) / C : 1;
     const size_t neq = ctx->cfg.num_equat;
+    // the segment buffer holds per step the state, t and, for RK4, the three
+    // stage inputs (SODECL_SEG_WIDTH in the adjoint kernel)
+    const size_t seg_width = ctx->cfg.solver == SODECL_RUNGE_KUTTA ? 4 * neq + 1 : neq + 1;
     const size_t need = io->grad_params || io->grad_y0
-                            ? sizeof(double) * n * (nckpt * (neq + 1) + static_cast<int64_t>(C) * (neq + 1))
+                            ? sizeof(double) * n * (nckpt * (neq + 1) + static_cast<int64_t>(C) * seg_width)
                             : 0;
     if (need > ctx->adj_scratch_bytes) {
         cudaFree(ctx->adj_scratch);
@@ -897,7 +899,6 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
         a.ckpt = base;
         a.ckpt_t = a.ckpt + nckpt * neq * n;
         a.seg = a.ckpt_t + nckpt * n;
-        a.seg_t = a.seg + static_cast<int64_t>(C) * neq * n;
         // the kernel writes gradients only when grad_p is set; give it a sink
         if (!a.grad_p) return ctx->fail(SODECL_ERR_INVALID_ARG, "adjoint: grad_params is required with grad_y0");
     }
