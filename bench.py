@@ -303,7 +303,9 @@ def main():
 
     # ---------------- companions: stable step, fp32, implicit midpoint
     extras = {}
-    if not a.no_extras and rank == 0:
+    # companions on single-GPU runs only: under torchrun they would hold every
+    # rank's GPU while rank 0 alone works
+    if not a.no_extras and world == 1:
         extras = companions(a, n, dev, stream)
         extras["gradient"] = gradient_companion(dev)
         extras["uneven_batch"] = batch_companion(dev)
