@@ -540,12 +540,21 @@ int sodecl_cuda_run(sodecl_ctx *ctx, double *out, int64_t out_len)
             SODECL_CUDA_TRY(ctx, cudaMalloc(&ctx->d_records, need));
             ctx->d_records_bytes = need;
         }
-        const int64_t groups = std::max<int64_t>(1, std::min<int64_t>(kMaxCopyGroups, ctx->nchunks));
+        // Launch groups of halving size (half the record intervals, a quarter,
+        // ...; the last takes the rest): each group's records are copied out on
+        // the second stream while later groups compute, and only the last, small
+        // group's copy is left exposed at the end.
+        std::vector<int64_t> first{0};
+        while (first.back() < ctx->nchunks) {
+            const int64_t rest = ctx->nchunks - first.back();
+            const bool last = static_cast<int64_t>(first.size()) == kMaxCopyGroups;
+            first.push_back(first.back() + (last ? rest : std::max<int64_t>(1, (rest + 1) / 2)));
+        }
+        if (first.size() == 1) first.push_back(0);  // no interval: one launch stores the final record
+        const int64_t groups = static_cast<int64_t>(first.size()) - 1;
         std::vector<cudaEvent_t> done(groups);
         for (auto &e : done) SODECL_CUDA_TRY(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
         EventGuard done_guard{done.data(), static_cast<int>(groups)};
-        std::vector<int64_t> first(groups + 1);
-        for (int64_t g = 0; g <= groups; ++g) first[g] = ctx->nchunks * g / groups;
         double *d_rec = static_cast<double *>(ctx->d_records);
         a.records = d_rec;
         for (int64_t g = 0; g < groups; ++g) {
