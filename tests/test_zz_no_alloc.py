@@ -22,9 +22,12 @@ from sodecl_b200.batch import Batch
 
 NOMINAL = np.array([120.0, 1.5, 0.0045, 0.05, 600.0, 9.0])
 Y0 = np.array([0.0, 0.0, 0.0, 0.0, 0.0, 2.0])
-# (system, solver, neq, npar, nnoi, dt)
+# (system, solver, neq, npar, nnoi, dt); the two wide Kuramoto classes run
+# several lanes per orbit, whose state lives in the kernel's dynamic shared
+# memory, which the allocation-free launch sizes as the regular one does
 CLASSES = [("kuramoto", "rk4", 8, 9, 0, 0.01), ("oculomotor", "rk4", 6, 6, 0, 1e-5),
-           ("oculomotor", "ie", 6, 6, 0, 1e-3), ("kuramoto", "se", 4, 9, 4, 0.01)]
+           ("oculomotor", "ie", 6, 6, 0, 1e-3), ("kuramoto", "se", 4, 9, 4, 0.01),
+           ("kuramoto", "rk4", 16, 17, 0, 0.01), ("kuramoto", "ie", 20, 21, 0, 0.01)]
 
 
 def build_batch():
@@ -59,7 +62,7 @@ def test_noalloc_batch_run_matches_regular_entry_point_twice():
     torch = pytest.importorskip("torch")
     if N.device_count() < 1:
         pytest.fail("no CUDA device")
-    per_class = [700, 900, 300, 500]
+    per_class = [700, 900, 300, 500, 400, 200]
     cls, steps, t0, y0, p, counters = class_grouped_items(per_class, 11)
 
     # the regular entry point: the library allocates and uploads
@@ -71,6 +74,7 @@ def test_noalloc_batch_run_matches_regular_entry_point_twice():
 
     # the allocation-free entry point: the caller owns every buffer
     b = build_batch()
+    assert max(b.lanes) > 1  # some classes run lanes per orbit
     dev = torch.device("cuda", 0)
     y_flat, p_flat = np.concatenate(y0), np.concatenate(p)
     counts = np.array(per_class, dtype=np.int64)
