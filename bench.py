@@ -260,9 +260,17 @@ def main():
     # orbits x records, which the traffic follows (it is the record stream)
     traffic = 137.3e6 * (n * nrec) / (262144 * 11) if (a.solver == "rk4" and a.precision == "fp64") else None
     algorithmic_bytes = nrec * 6 * n * 8 + n * (104 + 56)
+    hbm_gbs = algorithmic_bytes / (ms * 1e-3) / 1e9
+    hbm_peak = None
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            hbm_peak = float(json.load(f)["hbm_gbs"])
+    except (OSError, ValueError, KeyError):
+        pass
     roofline = {"bound": "fp64" if a.precision == "fp64" else "fp32", "achieved": achieved, "peak": peak_tflops,
                 "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if achieved else None, "traffic": traffic,
-                "algorithmic_bytes": algorithmic_bytes, "hbm_gbs": algorithmic_bytes / (ms * 1e-3) / 1e9,
+                "algorithmic_bytes": algorithmic_bytes, "hbm_gbs": hbm_gbs,
+                "hbm_frac_of_measured": (hbm_gbs / hbm_peak) if hbm_peak else None,
                 "peak_source": "measured on this GPU: FMA-chain microbenchmark (sodecl_cuda_fma_peak), 2 flops/FMA",
                 "ops_per_orbit_step": RK4_OPS_PER_ORBIT_STEP,
                 "fp64_pipe_active": "59.5 % of peak (ncu sm__pipe_fp64_cycles_active, 2^18-orbit x 1000-step "
