@@ -17,9 +17,11 @@
 // compiler hoists it out of the step loop and each quotient costs one
 // multiply and two FMAs instead of a full division.  Results are bit-for-bit
 // those of IEEE division (a NaN's payload aside).
-__device__ __forceinline__ double sodecl_div_rcp(double a, double b)
+// sodecl_div_by takes r = 1.0 / b from its caller, for a divisor that serves
+// several quotients (its reciprocal is then taken once); sodecl_div_rcp takes
+// the reciprocal itself.
+__device__ __forceinline__ double sodecl_div_by(double a, double b, double r)
 {
-    const double r = 1.0 / b;
     const double q = a * r;
     const double e = __fma_rn(-q, b, a);
     const double q2 = __fma_rn(e, r, q);
@@ -33,5 +35,7 @@ __device__ __forceinline__ double sodecl_div_rcp(double a, double b)
         return a + b;
     return a / b;
 }
+
+__device__ __forceinline__ double sodecl_div_rcp(double a, double b) { return sodecl_div_by(a, b, 1.0 / b); }
 
 #endif

@@ -49,6 +49,35 @@ __device__ __forceinline__ float sodecl_qdiv(float a, float b) { return a / b; }
 __device__ __forceinline__ sodecl_f64 sodecl_qdiv(sodecl_f64 a, sodecl_f64 b) { return sodecl_f64(a.v / b.v); }
 #endif
 
+// A pivot that divides twice (the banded solve's forward multiplier and back
+// substitution): in reciprocal-division programs its reciprocal is taken once
+// and each quotient finished from it (sodecl_div_by, the IEEE quotient's bits).
+#if SODECL_FAST_DIV
+__device__ __forceinline__ real_t sodecl_pivot_rcp(real_t d) { return sodecl_f64(1.0 / d.v); }
+__device__ __forceinline__ real_t sodecl_pdiv(real_t a, real_t d, real_t r) { return sodecl_f64(sodecl_div_by(a.v, d.v, r.v)); }
+#else
+__device__ __forceinline__ real_t sodecl_pivot_rcp(real_t d) { return d; }
+__device__ __forceinline__ real_t sodecl_pdiv(real_t a, real_t d, real_t) { return sodecl_qdiv(a, d); }
+#endif
+
+// 0 / d, IEEE: a zero with d's sign; NaN (through the division itself) for a
+// zero or NaN d.  The banded solve pads its super-diagonal with literal zeros.
+__device__ __forceinline__ real_t sodecl_zero_over(real_t d)
+{
+    if (d == (real_t)0 || d != d) return sodecl_qdiv((real_t)0, d);
+    return copysign((real_t)0, d);
+}
+
+// The implicit midpoint's stop test sqrt(norm) < _epsilon1_.  The square root
+// is correctly rounded and monotone, so the test holds exactly when norm is
+// below the least value whose root reaches _epsilon1_; the host computes that
+// bound (SODECL_L2_BOUND) whenever it is a normal number.
+#ifdef SODECL_L2_BOUND
+__device__ __forceinline__ bool sodecl_l2_below(real_t norm) { return norm < (real_t)SODECL_L2_BOUND; }
+#else
+__device__ __forceinline__ bool sodecl_l2_below(real_t norm) { return sqrt(norm) < (real_t)_epsilon1_; }
+#endif
+
 // Loops over equations unroll fully up to 16 equations (state, stages and
 // the Jacobian's bands then live in registers); wider systems keep their
 // arrays in local memory anyway, and full unrolling would only inflate the
@@ -148,16 +177,27 @@ __device__ __forceinline__ void sodecl_band_solve(real_t (*m)[_numeq_], real_t *
         lo[i] = (i < _numeq_ - 1) ? m[(i + 1) % _numeq_][i] : (real_t)0;
         d[i] = m[i][i];
     }
+    // rd[i]: the reciprocal of pivot i, for the pivots whose row below has a
+    // super-diagonal entry (i + 1 < _numeq_ - 2), which divide twice
+    real_t rd[_numeq_];
 #pragma unroll SODECL_EQ_UNROLL
     for (int i = 1; i < _numeq_; ++i) {
-        const real_t f = sodecl_qdiv(up[i], d[i - 1]);
+        real_t f;
+        if (i < _numeq_ - 2) {
+            rd[i - 1] = sodecl_pivot_rcp(d[i - 1]);
+            f = sodecl_pdiv(up[i], d[i - 1], rd[i - 1]);
+        } else {
+            f = sodecl_zero_over(d[i - 1]);
+        }
         d[i] = d[i] - f * lo[i - 1];
         v[i] = v[i] - f * v[i - 1];
     }
     x[_numeq_ - 1] = sodecl_qdiv(v[_numeq_ - 1], d[_numeq_ - 1]);
 #pragma unroll SODECL_EQ_UNROLL
-    for (int i = _numeq_ - 2; i >= 0; --i)
-        x[i] = sodecl_qdiv(v[i] - lo[i] * x[i + 1], d[i]);
+    for (int i = _numeq_ - 2; i >= 0; --i) {
+        const real_t num = v[i] - lo[i] * x[i + 1];
+        x[i] = (i + 1 < _numeq_ - 2) ? sodecl_pdiv(num, d[i], rd[i]) : sodecl_qdiv(num, d[i]);
+    }
 }
 
 // Implicit Euler (src/kernels/ie.cl:50-117) and implicit midpoint
@@ -165,54 +205,64 @@ __device__ __forceinline__ void sodecl_band_solve(real_t (*m)[_numeq_], real_t *
 //   IE: r = x - y - h f(t, x),         M = I - h J(x),          L1 test
 //   IM: r = x - y - h f(t, (y+x)/2),   M = I - (h/2) J((y+x)/2), L2 test
 // until the residual norm drops below _epsilon1_ or SODECL_NEWTON_MAX passes.
-// Returns the passes taken; sets `capped` when the limit was reached.
+//
+// One pass at iterate x: true when the residual norm is below _epsilon1_ (x
+// unchanged), else x <- x - M^-1 r and false.
+__device__ __forceinline__ bool sodecl_newton_pass(real_t h, real_t t, real_t *y, real_t *x, real_t *p)
+{
+    real_t f[_numeq_], r[_numeq_], dx[_numeq_];
+    real_t m[_numeq_][_numeq_];
+#if SODECL_SOLVER == 4
+    real_t mid[_numeq_];
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) mid[e] = (y[e] + x[e]) * (real_t)0.5;
+    sode_system(t, mid, f, p);
+#else
+    sode_system(t, x, f, p);
+#endif
+    real_t norm = 0;
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) {
+        r[e] = x[e] - y[e] - f[e] * h;
+#if SODECL_SOLVER == 4
+        norm = norm + r[e] * r[e];
+#else
+        norm = norm + fabs(r[e]);
+#endif
+    }
+#if SODECL_SOLVER == 4
+    if (sodecl_l2_below(norm)) return true;
+    calc_jacobian(mid, m, p);
+    const real_t scale = (real_t)(-0.50);
+#else
+    if (norm < (real_t)_epsilon1_) return true;
+    calc_jacobian(x, m, p);
+    const real_t scale = (real_t)(-1.00);
+#endif
+#pragma unroll SODECL_EQ_UNROLL
+    for (int i = 0; i < _numeq_; ++i) {
+#pragma unroll SODECL_EQ_UNROLL
+        for (int j = 0; j < _numeq_; ++j) m[i][j] = m[i][j] * scale * h;
+        m[i][i] = m[i][i] + 1;
+    }
+    sodecl_band_solve(m, r, dx);
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) x[e] = x[e] - dx[e];
+    return false;
+}
+
+// One step from y into ynew.  Returns the passes taken (residual evaluations);
+// sets `capped` when the limit was reached.
 __device__ __forceinline__ int sodecl_step_newton(real_t h, real_t t, real_t *y, real_t *ynew, real_t *p, int &capped)
 {
-    real_t x[_numeq_], f[_numeq_], r[_numeq_], dx[_numeq_];
-    real_t m[_numeq_][_numeq_];
+    real_t x[_numeq_];
 #pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) x[e] = y[e];
     int pass = 0;
     bool done = false;
 #pragma unroll 1
-    for (pass = 0; pass < SODECL_NEWTON_MAX; ++pass) {
-#if SODECL_SOLVER == 4
-        real_t mid[_numeq_];
-#pragma unroll SODECL_EQ_UNROLL
-        for (int e = 0; e < _numeq_; ++e) mid[e] = (y[e] + x[e]) * (real_t)0.5;
-        sode_system(t, mid, f, p);
-#else
-        sode_system(t, x, f, p);
-#endif
-        real_t norm = 0;
-#pragma unroll SODECL_EQ_UNROLL
-        for (int e = 0; e < _numeq_; ++e) {
-            r[e] = x[e] - y[e] - f[e] * h;
-#if SODECL_SOLVER == 4
-            norm = norm + r[e] * r[e];
-#else
-            norm = norm + fabs(r[e]);
-#endif
-        }
-#if SODECL_SOLVER == 4
-        if (sqrt(norm) < (real_t)_epsilon1_) { done = true; break; }
-        calc_jacobian(mid, m, p);
-        const real_t scale = (real_t)(-0.50);
-#else
-        if (norm < (real_t)_epsilon1_) { done = true; break; }
-        calc_jacobian(x, m, p);
-        const real_t scale = (real_t)(-1.00);
-#endif
-#pragma unroll SODECL_EQ_UNROLL
-        for (int i = 0; i < _numeq_; ++i) {
-#pragma unroll SODECL_EQ_UNROLL
-            for (int j = 0; j < _numeq_; ++j) m[i][j] = m[i][j] * scale * h;
-            m[i][i] = m[i][i] + 1;
-        }
-        sodecl_band_solve(m, r, dx);
-#pragma unroll SODECL_EQ_UNROLL
-        for (int e = 0; e < _numeq_; ++e) x[e] = x[e] - dx[e];
-    }
+    for (pass = 0; pass < SODECL_NEWTON_MAX; ++pass)
+        if (sodecl_newton_pass(h, t, y, x, p)) { done = true; break; }
     if (!done) capped = 1;
 #pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) ynew[e] = x[e];
@@ -381,6 +431,8 @@ __device__ __forceinline__ double sodecl_counter_plus(double counter, int c)
 
 #if SODECL_SOLVER == 3 || SODECL_SOLVER == 4
 // sodecl_band_solve on the shared band system (D, UP, LO, V) -> DX, by one lane.
+// (Plain quotients: with the loop rolled, sharing each pivot's reciprocal
+// between the two sweeps was measured slower here.)
 __device__ __forceinline__ void sodecl_lanes_band_solve(const sodecl_lanes_view &v)
 {
     real_t dprev = v.D[0], vprev = v.V[0];
@@ -451,7 +503,7 @@ __device__ __forceinline__ int sodecl_lanes_newton(real_t h, real_t t, const rea
 #endif
         }
 #if SODECL_SOLVER == 4
-        if (sqrt(norm) < (real_t)_epsilon1_) { done = true; break; }
+        if (sodecl_l2_below(norm)) { done = true; break; }
         const real_t scale = (real_t)(-0.50);
 #else
         if (norm < (real_t)_epsilon1_) { done = true; break; }
@@ -607,7 +659,126 @@ __device__ __forceinline__ void sodecl_store_record(const sodecl_args &a, int re
     if (!finite) flags |= SODECL_FLAG_NONFINITE;
 }
 
-#if SODECL_LANES == 1
+// The end of an orbit's launch: the closing record (on request), the state,
+// draw counter, Newton pass count and flags.
+__device__ __forceinline__ void sodecl_orbit_out(const sodecl_args &a, sodecl_i64 i, real_t t, const real_t *y,
+                                                 double counter, sodecl_i64 passes, int capped, int flags)
+{
+    if (a.write_final && a.records)
+        sodecl_store_record(a, a.chunk_end, i, y, flags);
+    a.t[i] = (double)t;
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) a.y[i * _numeq_ + e] = (double)y[e];
+#if SODECL_SOLVER == 0
+    a.counters[i] = counter;
+#endif
+    (void)counter;
+    if (capped) flags |= SODECL_FLAG_NEWTON_CAP;
+    if (a.newton_passes) a.newton_passes[i] += passes;
+    if (a.flags && flags) a.flags[i] |= flags;
+}
+
+// [lo of part k, when n items are split into parts parts as evenly as possible)
+__device__ __forceinline__ sodecl_i64 sodecl_split(sodecl_i64 n, sodecl_i64 k, sodecl_i64 parts)
+{
+    const sodecl_i64 q = n / parts, r = n % parts;
+    return k * q + (k < r ? k : r);
+}
+
+#if SODECL_LANES == 1 && (SODECL_SOLVER == 3 || SODECL_SOLVER == 4)
+// Implicit solvers, one thread per orbit.  The orbits of a warp need
+// different numbers of Newton passes per step, and a few need hundreds in
+// some step (the pass limit), so this kernel keeps the warp's lanes busy two
+// ways:
+//  - Newton passes drive the loop, not steps: a lane whose iteration has
+//    converged commits its step and starts the next one at the following
+//    pass (sodecl_step_newton's arithmetic, in the same order);
+//  - each warp owns a contiguous range of the launch's orbits, and a lane
+//    whose orbit is done takes the range's next orbit (a ballot hands them
+//    out in lane order), so a slow orbit holds up no other.
+// The host launches at most the blocks that are resident at once, so each
+// warp's range holds several orbits per lane.  Any block size works: the warp
+// operations name only the lanes that exist.
+extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS)
+sodecl_orbits(const sodecl_args a)
+{
+    const int lane = threadIdx.x % 32;
+    const int in_warp = min(32, (int)blockDim.x - (int)(threadIdx.x / 32) * 32);
+    const unsigned wmask = in_warp == 32 ? 0xffffffffu : (1u << in_warp) - 1u;
+    const sodecl_i64 warps_per_block = (blockDim.x + 31) / 32;
+    const sodecl_i64 nwarps = (sodecl_i64)gridDim.x * warps_per_block;
+    const sodecl_i64 w = (sodecl_i64)blockIdx.x * warps_per_block + threadIdx.x / 32;
+    sodecl_i64 next = sodecl_split(a.n, w, nwarps);
+    const sodecl_i64 hi = sodecl_split(a.n, w + 1, nwarps);
+
+    real_t y[_numeq_], x[_numeq_];
+    real_t p[SODECL_NPAR_ALLOC];
+    real_t t = 0;
+    sodecl_i64 i = 0, passes = 0;
+    int c = 0, s = 0, pass = 0, flags = 0, capped = 0;
+    bool active = false;
+#pragma unroll 1
+    for (;;) {
+        // hand the range's next orbits to the idle lanes
+        const unsigned idle = __ballot_sync(wmask, !active);
+        if (idle != 0u && next < hi) {
+            const sodecl_i64 mine = next + __popc(idle & ((1u << lane) - 1u));
+            next += __popc(idle);
+            if (!active && mine < hi) {
+                i = mine;
+                t = (real_t)a.t[i];
+#pragma unroll SODECL_EQ_UNROLL
+                for (int e = 0; e < _numeq_; ++e) y[e] = x[e] = (real_t)a.y[i * _numeq_ + e];
+#pragma unroll SODECL_PAR_UNROLL
+                for (int k = 0; k < _numpar_; ++k) p[k] = (real_t)__ldg(a.p + i * _numpar_ + k);
+                c = a.chunk_begin;
+                s = pass = flags = capped = 0;
+                passes = 0;
+                if (c < a.chunk_end) {
+                    if (a.records) sodecl_store_record(a, c, i, y, flags);
+                    active = true;
+                } else {
+                    sodecl_orbit_out(a, i, t, y, 0.0, passes, capped, flags);
+                }
+            }
+        }
+        if (!__any_sync(wmask, active)) {
+            if (next >= hi) break;
+            continue;
+        }
+        // Newton passes with every lane's parameters fixed (what depends on
+        // them alone is computed once, out of this loop), until a lane is idle
+        // while the range has orbits left, or every lane is done
+#pragma unroll 1
+        for (;;) {
+            if (active) {
+                // a pass limit below one takes no pass: the step is capped at once
+                const bool done = SODECL_NEWTON_MAX >= 1 && sodecl_newton_pass(_m_dt_, t, y, x, p);
+                if (SODECL_NEWTON_MAX >= 1) ++pass;
+                if (done || pass >= SODECL_NEWTON_MAX) {
+                    if (!done) capped = 1;
+                    passes += pass;
+                    pass = 0;
+                    t = t + _m_dt_;
+#pragma unroll SODECL_EQ_UNROLL
+                    for (int e = 0; e < _numeq_; ++e) y[e] = x[e];
+                    if (++s == _numsteps_) {
+                        s = 0;
+                        if (++c < a.chunk_end) {
+                            if (a.records) sodecl_store_record(a, c, i, y, flags);
+                        } else {
+                            sodecl_orbit_out(a, i, t, y, 0.0, passes, capped, flags);
+                            active = false;
+                        }
+                    }
+                }
+            }
+            const unsigned now_idle = __ballot_sync(wmask, !active);
+            if (now_idle == wmask || (now_idle != 0u && next < hi)) break;
+        }
+    }
+}
+#elif SODECL_LANES == 1
 extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS)
 sodecl_orbits(const sodecl_args a)
 {
@@ -640,18 +811,7 @@ sodecl_orbits(const sodecl_args a)
         for (int s = 0; s < _numsteps_; ++s)
             sodecl_advance(t, y, p, gid, counter, passes, capped);
     }
-    if (a.write_final && a.records)
-        sodecl_store_record(a, a.chunk_end, i, y, flags);
-
-    a.t[i] = (double)t;
-#pragma unroll SODECL_EQ_UNROLL
-    for (int e = 0; e < _numeq_; ++e) a.y[i * _numeq_ + e] = (double)y[e];
-#if SODECL_SOLVER == 0
-    a.counters[i] = counter;
-#endif
-    if (capped) flags |= SODECL_FLAG_NEWTON_CAP;
-    if (a.newton_passes) a.newton_passes[i] += passes;
-    if (a.flags && flags) a.flags[i] |= flags;
+    sodecl_orbit_out(a, i, t, y, counter, passes, capped, flags);
 }
 #else  // SODECL_LANES > 1
 __device__ __forceinline__ void sodecl_lanes_store(const sodecl_args &a, int rec, sodecl_i64 i, const real_t *yown,

@@ -16,10 +16,12 @@
 #include <unistd.h>
 
 #include <cctype>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <fstream>
+#include <limits>
 #include <mutex>
 #include <regex>
 #include <sstream>
@@ -325,6 +327,37 @@ std::string print_like_reference(double x)
     return ss.str();
 }
 
+namespace {
+
+// The least t >= 0 whose correctly rounded square root (in T, double or float)
+// reaches eps, as an exact hexadecimal literal: sqrt(norm) < eps holds exactly
+// when norm < t, the root being monotone.  Empty when eps is not positive and
+// finite or t is not a normal number (the solvers then keep the root).
+template <typename T>
+std::string l2_bound_literal(T eps)
+{
+    if (!(eps > 0) || !std::isfinite(eps)) return "";
+    T t = eps * eps;
+    if (!std::isfinite(t) || t < std::numeric_limits<T>::min()) return "";
+    while (t > 0 && std::sqrt(t) >= eps) t = std::nextafter(t, T(0));
+    while (std::sqrt(t) < eps) t = std::nextafter(t, std::numeric_limits<T>::infinity());
+    if (!std::isfinite(t) || t < std::numeric_limits<T>::min()) return "";
+    char buf[64];
+    std::snprintf(buf, sizeof buf, "%a", static_cast<double>(t));
+    return std::string(buf) + (sizeof(T) == sizeof(float) ? "f" : "");
+}
+
+}  // namespace
+
+std::string l2_bound_define(double newton_tol, bool fp32)
+{
+    // the tolerance as the program's _epsilon1_ text reads it
+    const std::string text = print_like_reference(newton_tol);
+    const std::string lit = fp32 ? l2_bound_literal(std::strtof(text.c_str(), nullptr))
+                                 : l2_bound_literal(std::strtod(text.c_str(), nullptr));
+    return lit.empty() ? std::string() : "#define SODECL_L2_BOUND " + lit + "\n";
+}
+
 std::string suffix_float_literals(const std::string &src)
 {
     return scan_code(src, suffix_in_code, true);
@@ -384,6 +417,7 @@ std::string assemble(const ProgramSpec &spec, const std::string &system_src, con
     std::string eps = print_like_reference(spec.newton_tol);
     if (spec.fp32) eps = suffix_in_code(eps);
     s << "#define _epsilon1_ " << eps << "\n";
+    s << l2_bound_define(spec.newton_tol, spec.fp32);
     if (spec.fp32) s << "#define double float\n";
     else if (spec.fast_div) s << "#define double sodecl_f64\n";
     s << "#line 1 \"system.cl\"\n";
@@ -496,8 +530,8 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
     s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n" << kBatchSrc << "\n";
     static const char *per_class[] = {"SODECL_SOLVER", "SODECL_HAS_JACOBIAN", "SODECL_HAS_STOCH", "SODECL_NEWTON_MAX",
                                       "_numnoi_", "_numsteps_", "_m_dt_", "_numeq_", "_numpar_", "_epsilon1_",
-                                      "_listsize_", "SODECL_BATCH_CLASS_BODY", "SODECL_LANES", "SODECL_HAS_ROW",
-                                      "SODECL_HAS_STOCH_ROW", "SODECL_HAS_JAC_BAND"};
+                                      "SODECL_L2_BOUND", "_listsize_", "SODECL_BATCH_CLASS_BODY", "SODECL_LANES",
+                                      "SODECL_HAS_ROW", "SODECL_HAS_STOCH_ROW", "SODECL_HAS_JAC_BAND"};
     for (size_t k = 0; k < classes.size(); ++k) {
         const ProgramSpec &sp = classes[k].spec;
         const std::string &src = classes[k].system_src;
@@ -519,6 +553,7 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
         s << "#define _numeq_ " << sp.num_equat << "\n";
         s << "#define _numpar_ " << sp.num_params << "\n";
         s << "#define _epsilon1_ " << print_like_reference(sp.newton_tol) << "\n";
+        s << l2_bound_define(sp.newton_tol, false);
         s << "namespace sodecl_cls_" << k << " {\n";
         if (fast_div) s << "#define double sodecl_f64\n";
         s << "#line 1 \"class" << k << ".cl\"\n" << relax_parameter_bounds(src) << "\n";
@@ -569,6 +604,7 @@ std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, in
     s << "#define _numeq_ " << spec.num_equat << "\n";
     s << "#define _numpar_ " << spec.num_params << "\n";
     s << "#define _epsilon1_ " << print_like_reference(spec.newton_tol) << "\n";
+    s << l2_bound_define(spec.newton_tol, false);
     const std::string user = relax_parameter_bounds(src);
     const std::vector<std::string> macros = defined_macros(src);
     if (fast_div) s << "#define double sodecl_f64\n";

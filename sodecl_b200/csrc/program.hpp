@@ -53,6 +53,9 @@ SystemTraits inspect_system(const std::string &src);
 // `dt` exactly as the reference writes it into `#define _m_dt_`: a default
 // std::ostream, i.e. %g with 6 significant digits (src/sodeclmgr.cpp:356-367).
 std::string print_like_reference(double x);
+// "#define SODECL_L2_BOUND <t>\n": the exact bound for the implicit midpoint's
+// stop test sqrt(norm) < tol (norm < t), or "" where it is not a normal number.
+std::string l2_bound_define(double newton_tol, bool fp32);
 
 // Every unsuffixed floating literal outside comments, strings and character
 // constants gets an `f` suffix (fp32 programs).

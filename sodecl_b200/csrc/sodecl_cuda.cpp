@@ -262,7 +262,25 @@ Geometry geometry(const sodecl_cfg &c, int64_t n)
 int launch_kernel(sodecl_ctx *ctx, cudaKernel_t kernel, const sodecl_cfg &c, const DeviceArgs &a, cudaStream_t stream)
 {
     if (a.n <= 0) return SODECL_OK;
-    const Geometry g = geometry(c, a.n);
+    Geometry g = geometry(c, a.n);
+    if (lanes_of(c) == 1 && (c.solver == SODECL_IMPLICIT_EULER || c.solver == SODECL_IMPLICIT_MIDPOINT)) {
+        // the implicit kernel's warps share out ranges of orbits among their
+        // lanes: give every lane the same number of orbits, the fewest that
+        // fit the threads resident at once, and launch just the blocks for that
+        int per_sm = 0, dev = 0, sms = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void *>(kernel), g.block,
+                                                          0) != cudaSuccess ||
+            cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            per_sm = sms = 0;
+        }
+        const int64_t resident = static_cast<int64_t>(per_sm) * sms * g.block;
+        if (resident > 0 && a.n > resident) {
+            const int64_t per_lane = (a.n + resident - 1) / resident;
+            g.grid = (a.n + per_lane * g.block - 1) / (per_lane * g.block);
+        }
+    }
     if (g.grid > 0x7fffffffLL) return ctx->fail(SODECL_ERR_INVALID_ARG, "too many orbits for one launch");
     if (g.shared > kLanesSharedCap)
         return ctx->fail(SODECL_ERR_UNSUPPORTED, "one orbit's state, parameters and noise exceed the shared memory of a "
@@ -297,6 +315,12 @@ ProgramSpec make_spec(const sodecl_cfg &c)
     const int block = c.local_group_size > 0 ? c.local_group_size : kDefaultBlock;
     spec.block_max = std::max(256, c.lanes_per_orbit > 1 ? (block + 31) / 32 * 32 : block);
     spec.min_blocks = c.min_blocks_per_sm;
+    // implicit solvers, one thread per orbit: by default at most 128 registers
+    // a thread (four blocks of 128 threads on an SM); above that the Newton
+    // pass's hoisted terms took more registers than the occupancy they cost
+    if (spec.min_blocks == 0 && lanes_of(c) == 1 &&
+        (c.solver == SODECL_IMPLICIT_EULER || c.solver == SODECL_IMPLICIT_MIDPOINT))
+        spec.min_blocks = std::max(1, 65536 / (spec.block_max * 128));
     spec.fast_div = c.division == SODECL_DIV_RECIPROCAL;
     spec.lanes = lanes_of(c);
     return spec;
@@ -702,6 +726,9 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
     // lanes per orbit: up to the first power of two >= the equations
     const auto traits = sodecl_b200::inspect_system(ctx->system_src);
     const int solver = ctx->cfg.solver;
+    // implicit solvers run under a register cap by default (min_blocks 0); 1 lifts it
+    if (solver == SODECL_IMPLICIT_EULER || solver == SODECL_IMPLICIT_MIDPOINT)
+        cands.push_back({128, 1, ctx->cfg.precision == SODECL_FP64 ? SODECL_DIV_RECIPROCAL : SODECL_DIV_IEEE, 1});
     const bool row_ok = lanes_supported(traits, solver);
     if (row_ok) {
         for (int l = 2; l <= 32 && l / 2 < ctx->cfg.num_equat; l *= 2) {

@@ -103,6 +103,37 @@ def test_compile_every_solver_without_gpu(solver, precision):
     N.lib.sodecl_cuda_destroy(ctx)
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("tol", [1e-7, 1e-10, 3e-5, 1e-3, 0.5, 7.25e-13])
+def test_midpoint_stop_bound_is_exact(precision, tol):
+    """The implicit midpoint stops when sqrt(norm) < tol (src/kernels/im.cl);
+    the program tests norm < t instead, with t from the host: the least value
+    whose correctly rounded square root reaches tol.  Both tests agree for every
+    norm exactly when sqrt(t) >= tol > sqrt(t's predecessor)."""
+    rc, ctx = _create(solver=N.IMPLICIT_MIDPOINT, precision=precision, newton_tol=tol)
+    assert rc == N.OK
+    assert _compile(ctx, open(system_path("oculomotor")).read()) == N.OK, N.last_error(ctx)
+    text = N.program_source(ctx)
+    N.lib.sodecl_cuda_destroy(ctx)
+    m = re.search(r"#define SODECL_L2_BOUND (\S+)", text)
+    assert m, "no bound in the program"
+    ft = np.float32 if precision else np.float64
+    t = ft(float.fromhex(m.group(1).rstrip("f")))
+    # tol as the program's _epsilon1_ literal reads it (float literals parse straight to float)
+    eps_text = re.search(r"#define _epsilon1_ (\S+)", text).group(1).rstrip("f").encode()
+    libc = C.CDLL(None)
+    libc.strtof.restype, libc.strtod.restype = C.c_float, C.c_double
+    libc.strtof.argtypes = libc.strtod.argtypes = [C.c_char_p, C.c_void_p]
+    eps = ft(libc.strtof(eps_text, None) if precision else libc.strtod(eps_text, None))
+    assert np.sqrt(t) >= eps and np.sqrt(np.nextafter(t, ft(0))) < eps
+    v = t
+    for _ in range(64):  # and on either side of it
+        v = np.nextafter(v, ft(0))
+    for _ in range(128):
+        assert (np.sqrt(v) < eps) == (v < t)
+        v = np.nextafter(v, ft(np.inf))
+
+
 def test_fp32_program_rewrites_literals():
     rc, ctx = _create(precision=1)
     assert _compile(ctx, open(system_path("oculomotor")).read()) == N.OK

@@ -20,7 +20,8 @@ Y0 = np.array([0.0, 0.0, 0.0, 0.0, 0.0, 2.0])
 # (system, solver, neq, npar, nnoi, dt)
 CLASSES = [("kuramoto", "euler", 4, 5, 0, 0.01), ("kuramoto", "rk4", 16, 17, 0, 0.01),
            ("kuramoto", "ie", 8, 9, 0, 0.01), ("oculomotor", "rk4", 6, 6, 0, 1e-5),
-           ("oculomotor", "ie", 6, 6, 0, 1e-3), ("kuramoto", "se", 5, 11, 5, 0.01)]
+           ("oculomotor", "ie", 6, 6, 0, 1e-3), ("kuramoto", "se", 5, 11, 5, 0.01),
+           ("oculomotor", "im", 6, 6, 0, 1e-3)]
 
 
 def make_batch(fmad=True, classes=CLASSES):

@@ -384,7 +384,8 @@ def test_reciprocal_quotient_equals_ieee_division():
 
 @pytest.mark.parametrize("fmad", [0, 1])
 @pytest.mark.parametrize("system,solver,dt", [("oculomotor", "rk4", 1e-5), ("oculomotor", "ie", 1e-3),
-                                              ("oculomotor", "euler", 1e-6), ("kuramoto", "se", 0.01)])
+                                              ("oculomotor", "im", 1e-3), ("oculomotor", "euler", 1e-6),
+                                              ("kuramoto", "se", 0.01)])
 def test_division_modes_give_identical_records(system, solver, dt, fmad):
     n = 2048
     if system == "oculomotor":
