@@ -372,6 +372,47 @@ def test_cpp_sodeclmgr_drop_in(tmp_path):
     np.testing.assert_array_equal(filemode, np.fromfile(out_file))
 
 
+@pytest.mark.parametrize("solver", ["ie", "im"])
+def test_implicit_kernel_launch_shapes_agree(solver):
+    """The implicit kernel's warps hand out ranges of orbits to their lanes, and
+    the host launches only as many blocks as give each lane the fewest orbits
+    that fit the resident threads.  Block sizes that are not a multiple of 32
+    (partial warps), more orbits than resident threads (several orbits a
+    lane), the register cap lifted, and sodecl_cuda_launch on a slice of the
+    orbits in two interval ranges all give the same records, pass counts and
+    flags, bit for bit."""
+    import torch
+
+    n = 150000  # above the resident threads of a B200 at 128 registers
+    t0, y0, p = oculomotor_inputs(n, 31)
+    kw = dict(dt=1e-3, tspan=60e-3, ksteps=20, neq=6, npar=6)
+    outs = []
+    for block, minb in ((128, 0), (100, 0), (33, 0), (512, 0), (128, 1)):
+        with Integrator(system_path("oculomotor"), solver, orbits=n, block=block, min_blocks=minb, **kw) as sim:
+            sim.upload(t0, y0, p)
+            rec = sim.run()
+            passes, flags = sim.status()
+        outs.append((rec, passes, flags))
+    for rec, passes, flags in outs[1:]:
+        np.testing.assert_array_equal(rec, outs[0][0])
+        np.testing.assert_array_equal(passes, outs[0][1])
+        np.testing.assert_array_equal(flags, outs[0][2])
+    # a slice of the orbits through the device launch
+    lo, hi = 4321, 104321
+    dev = torch.device("cuda", 0)
+    with Integrator(system_path("oculomotor"), solver, orbits=n, **kw) as sim:
+        T = lambda x: torch.tensor(x, device=dev)  # noqa: E731
+        td, yd, pd = T(t0[lo:hi]), T(y0[lo:hi]), T(p[lo:hi])
+        nchunks = sim.num_chunks
+        rec = torch.full((nchunks + 1, 6, n), float("nan"), dtype=torch.float64, device=dev)
+        for c0, c1 in ((0, 1), (1, nchunks)):  # the second launch continues from the first's state
+            sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(), records=rec.data_ptr(), n=hi - lo,
+                       orbit_offset=lo, rec_stride=n, rec_col0=lo, chunk_begin=c0, chunk_end=c1,
+                       write_final=(c1 == nchunks), stream=torch.cuda.current_stream(dev).cuda_stream)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(rec[:, :, lo:hi].cpu().numpy(), outs[0][0][:, :, lo:hi])
+
+
 # --------------------------------------------------------------------------
 # the reciprocal quotient
 
