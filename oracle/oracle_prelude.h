@@ -31,6 +31,11 @@
 #define M_PI 3.14159265358979323846
 #endif
 
+/* OpenCL C's sincos(x, &c): returns sin(x), stores cos(x) */
+static inline double sodecl_sincos_d(double x, double *c) { *c = cos(x); return sin(x); }
+static inline float sodecl_sincos_f(float x, float *c) { *c = cos(x); return sin(x); }
+#define sincos(x, c) _Generic((x), float: sodecl_sincos_f, default: sodecl_sincos_d)(x, c)
+
 extern int g_sodecl_numeq;
 extern int g_sodecl_numpar;
 extern int g_sodecl_numnoi;

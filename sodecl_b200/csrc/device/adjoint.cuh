@@ -138,6 +138,7 @@ __device__ __forceinline__ sodecl_ad log(const sodecl_ad &a) { return sodecl_ad_
 __device__ __forceinline__ sodecl_ad sqrt(const sodecl_ad &a) { const double s = ::sqrt(a.v); return sodecl_ad_un(s, a, 0.5 / s); }
 __device__ __forceinline__ sodecl_ad sin(const sodecl_ad &a) { return sodecl_ad_un(::sin(a.v), a, ::cos(a.v)); }
 __device__ __forceinline__ sodecl_ad cos(const sodecl_ad &a) { return sodecl_ad_un(::cos(a.v), a, -::sin(a.v)); }
+__device__ __forceinline__ sodecl_ad sincos(const sodecl_ad &a, sodecl_ad *c) { *c = cos(a); return sin(a); }
 __device__ __forceinline__ sodecl_ad tan(const sodecl_ad &a) { const double c = ::cos(a.v); return sodecl_ad_un(::tan(a.v), a, 1.0 / (c * c)); }
 __device__ __forceinline__ sodecl_ad tanh(const sodecl_ad &a) { const double h = ::tanh(a.v); return sodecl_ad_un(h, a, 1.0 - h * h); }
 __device__ __forceinline__ sodecl_ad sinh(const sodecl_ad &a) { return sodecl_ad_un(::sinh(a.v), a, ::cosh(a.v)); }

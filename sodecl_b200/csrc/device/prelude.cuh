@@ -127,7 +127,13 @@ __device__ __forceinline__ double mix(double a, double b, double t) { return a +
 __device__ __forceinline__ float mix(float a, float b, float t) { return a + (b - a) * t; }
 __device__ __forceinline__ double sign(double x) { return x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : (x == x ? 0.0 : x)); }
 __device__ __forceinline__ float sign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : (x == x ? 0.0f : x)); }
+// OpenCL C's sincos: returns sin(x) and stores cos(x), each the same value as
+// sin(x) and cos(x) alone, with one argument reduction for both (CUDA's
+// three-argument sincos stays available)
+__device__ __forceinline__ double sincos(double x, double *c) { double s; ::sincos(x, &s, c); return s; }
+__device__ __forceinline__ float sincos(float x, float *c) { float s; ::sincosf(x, &s, c); return s; }
 #if SODECL_FAST_DIV
+__device__ __forceinline__ sodecl_f64 sincos(sodecl_f64 x, sodecl_f64 *c) { double s; ::sincos(x.v, &s, &c->v); return sodecl_f64(s); }
 __device__ __forceinline__ sodecl_f64 mad(sodecl_f64 a, sodecl_f64 b, sodecl_f64 c) { return a * b + c; }
 __device__ __forceinline__ sodecl_f64 pown(sodecl_f64 x, int n) { return pow(x, sodecl_f64((double)n)); }
 __device__ __forceinline__ sodecl_f64 clamp(sodecl_f64 x, sodecl_f64 lo, sodecl_f64 hi) { return fmin(fmax(x, lo), hi); }

@@ -27,6 +27,7 @@
 //   SODECL_HAS_ROW, SODECL_HAS_STOCH_ROW, SODECL_HAS_JAC_BAND  the system
 //                        file defines sode_system_row / sode_system_stoch_row /
 //                        calc_jacobian_band
+//   SODECL_HAS_ROW_BAND  the system file defines sode_system_row_band
 
 #ifndef SODECL_MIN_BLOCKS
 #define SODECL_MIN_BLOCKS 1
@@ -486,11 +487,23 @@ __device__ __forceinline__ int sodecl_lanes_newton(real_t h, real_t t, const rea
 #else
         real_t *at = v.A;
 #endif
+#if SODECL_HAS_ROW_BAND
+        // the row's right-hand side and its band entries from one evaluation
+        // (the Jacobian is taken at the residual's point), used if the pass
+        // does not converge
+        real_t bands[SODECL_ROWS][3];
+#pragma unroll
+        for (int k = 0; k < SODECL_ROWS; ++k) {
+            const int row = v.lane + k * SODECL_LANES;
+            if (row < _numeq_) r[k] = x[k] - yown[k] - sode_system_row_band(row, t, at, bands[k], v.P) * h;
+        }
+#else
 #pragma unroll
         for (int k = 0; k < SODECL_ROWS; ++k) {
             const int row = v.lane + k * SODECL_LANES;
             if (row < _numeq_) r[k] = x[k] - yown[k] - sode_system_row(row, t, at, v.P) * h;
         }
+#endif
         // the residual norm in row order, every lane of the group the same
         real_t norm = 0;
 #pragma unroll
@@ -513,8 +526,12 @@ __device__ __forceinline__ int sodecl_lanes_newton(real_t h, real_t t, const rea
         for (int k = 0; k < SODECL_ROWS; ++k) {
             const int row = v.lane + k * SODECL_LANES;
             if (row < _numeq_) {
+#if SODECL_HAS_ROW_BAND
+                const real_t *band = bands[k];
+#else
                 real_t band[3];
                 calc_jacobian_band(row, at, band, v.P);
+#endif
                 real_t d = band[1] * scale * h;
                 d = d + 1;
                 v.D[row] = d;

@@ -374,6 +374,7 @@ SystemTraits inspect_system(const std::string &src)
     t.has_row = defines_function(stripped, "sode_system_row");
     t.has_stoch_row = defines_function(stripped, "sode_system_stoch_row");
     t.has_jac_band = defines_function(stripped, "calc_jacobian_band");
+    t.has_row_band = defines_function(stripped, "sode_system_row_band");
     t.has_vjp = defines_function(stripped, "calc_vjp");
     t.uses_listsize = std::regex_search(stripped, std::regex("\\b_listsize_\\b"));
     return t;
@@ -402,6 +403,7 @@ std::string assemble(const ProgramSpec &spec, const std::string &system_src, con
     s << "#define SODECL_HAS_ROW " << (traits.has_row ? 1 : 0) << "\n";
     s << "#define SODECL_HAS_STOCH_ROW " << (traits.has_stoch_row ? 1 : 0) << "\n";
     s << "#define SODECL_HAS_JAC_BAND " << (traits.has_jac_band ? 1 : 0) << "\n";
+    s << "#define SODECL_HAS_ROW_BAND " << (traits.has_row_band ? 1 : 0) << "\n";
     s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n";
     // the reference's program defines (src/sodeclmgr.cpp:379-430); _listsize_
     // only when the system file names it, so one program serves every size
@@ -531,7 +533,8 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
     static const char *per_class[] = {"SODECL_SOLVER", "SODECL_HAS_JACOBIAN", "SODECL_HAS_STOCH", "SODECL_NEWTON_MAX",
                                       "_numnoi_", "_numsteps_", "_m_dt_", "_numeq_", "_numpar_", "_epsilon1_",
                                       "SODECL_L2_BOUND", "_listsize_", "SODECL_BATCH_CLASS_BODY", "SODECL_LANES",
-                                      "SODECL_HAS_ROW", "SODECL_HAS_STOCH_ROW", "SODECL_HAS_JAC_BAND"};
+                                      "SODECL_HAS_ROW", "SODECL_HAS_STOCH_ROW", "SODECL_HAS_JAC_BAND",
+                                      "SODECL_HAS_ROW_BAND"};
     for (size_t k = 0; k < classes.size(); ++k) {
         const ProgramSpec &sp = classes[k].spec;
         const std::string &src = classes[k].system_src;
@@ -546,6 +549,7 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
         s << "#define SODECL_HAS_ROW " << (tr.has_row ? 1 : 0) << "\n";
         s << "#define SODECL_HAS_STOCH_ROW " << (tr.has_stoch_row ? 1 : 0) << "\n";
         s << "#define SODECL_HAS_JAC_BAND " << (tr.has_jac_band ? 1 : 0) << "\n";
+        s << "#define SODECL_HAS_ROW_BAND " << (tr.has_row_band ? 1 : 0) << "\n";
         s << "#define _numnoi_ " << sp.num_noi << "\n";
         s << "#define _listsize_ " << sp.list_size << "\n";
         s << "#define _numsteps_ 1\n";

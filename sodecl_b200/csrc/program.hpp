@@ -44,6 +44,7 @@ struct SystemTraits {
     bool has_row = false;        // sode_system_row (one equation's right-hand side)
     bool has_stoch_row = false;  // sode_system_stoch_row
     bool has_jac_band = false;   // calc_jacobian_band (row i's entries in columns i-1, i, i+1)
+    bool has_row_band = false;   // sode_system_row_band (a row's right-hand side and band together)
     bool has_vjp = false;        // calc_vjp (v^T df/dy and v^T df/dp), used by the adjoint
     bool uses_listsize = false;
 };

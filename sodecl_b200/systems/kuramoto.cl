@@ -18,6 +18,7 @@
  * (columns i-1, i, i+1), evaluated exactly as `sode_system`,
  * `sode_system_stoch` and `calc_jacobian` evaluate them; with them, several
  * lanes of a warp can share one orbit (lanes per orbit).
+ * `sode_system_row_band` gives a row's right-hand side and band together.
  */
 
 void sode_system(double t, double y[_numeq_], double yout[_numeq_], double p[_numpar_])
@@ -87,6 +88,43 @@ void calc_jacobian_band(int i, double y[_numeq_], double band[3], double p[_nump
 		}
 	}
 	band[1] = diag;
+}
+
+/* sode_system_row and calc_jacobian_band of row i in one evaluation, with
+ * sin and cos of each difference from one sincos: returns yout[i], fills
+ * band[0..2] (columns i-1, i, i+1); both are the same values those two
+ * functions give.  The implicit solvers with lanes per orbit use it (each
+ * Newton pass needs the row and, until it converges, the band at the same
+ * point). */
+double sode_system_row_band(int i, double t, double y[_numeq_], double band[3], double p[_numpar_])
+{
+	double scale = (double)(p[0] / (double)(_numeq_));
+	double coupling = 0;
+	double diag = 0;
+	band[0] = 0;
+	band[2] = 0;
+	for (int j = 0; j < _numeq_; j++)
+	{
+		double cosine;
+		double sine = sincos(y[j] - y[i], &cosine);
+		coupling = coupling + sine;
+		double c = scale * cosine;
+		if (j == i - 1)
+		{
+			band[0] = c;
+		}
+		if (j == i + 1)
+		{
+			band[2] = c;
+		}
+		if (j != i)
+		{
+			diag = diag - c;
+		}
+	}
+	band[1] = diag;
+	coupling = coupling * (double)(p[0] / (double)(_numeq_));
+	return coupling + p[i + 1];
 }
 
 void sode_system_stoch(double t, double y[_numeq_], double stoch[_numeq_], double p[_numpar_], double noise[_numnoi_])

@@ -114,6 +114,32 @@ def test_autotune_considers_lanes_and_keeps_results():
 # ---------------------------------------------------------------- no GPU needed
 
 
+@pytest.mark.gpu
+@pytest.mark.parametrize("N_osc,solver,lanes,precision", [(64, "ie", 32, "fp64"), (16, "im", 8, "fp64"),
+                                                          (33, "ie", 32, "fp32"), (20, "im", 16, "fp64")])
+def test_row_band_hook_gives_the_same_records(N_osc, solver, lanes, precision):
+    """With sode_system_row_band in the system file, a Newton pass takes a row's
+    right-hand side and band from one evaluation (sin and cos from one
+    sincos); without it, from sode_system_row and calc_jacobian_band.  The
+    records, pass counts and flags are the same, with FMA contraction on."""
+    n = 257
+    t0, y0, p, _ = kuramoto_inputs(n, N_osc, 0, 7 * N_osc + lanes)
+    src = open(system_path("kuramoto")).read()
+    assert "sode_system_row_band(" in src
+    outs = []
+    for text in (src, src.replace("sode_system_row_band(", "unused_row_band(")):
+        with Integrator(None, solver, orbits=n, lanes=lanes, dt=0.01, tspan=1.0, ksteps=10, neq=N_osc,
+                        npar=p.shape[1], precision=precision, newton_tol=1e-7 if precision == "fp64" else 1e-4,
+                        system_src=text) as sim:
+            assert ("#define SODECL_HAS_ROW_BAND 1" in sim.program_source) == (text is src)
+            sim.upload(t0, y0, p)
+            rec = sim.run()
+            passes, flags = sim.status()
+        outs.append((rec, passes, flags))
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)
+
+
 def _create(solver, lanes, system="kuramoto", neq=8, npar=9, nnoi=0, drop=None):
     cfg = N.Cfg()
     N.lib.sodecl_cfg_init(C.byref(cfg))
@@ -159,4 +185,12 @@ def test_lanes_program_compiles_without_gpu():
     assert rc == N.OK
     src = N.program_source(ctx)
     assert "#define SODECL_LANES 16" in src and "#define SODECL_HAS_STOCH_ROW 1" in src
+    N.lib.sodecl_cuda_destroy(ctx)
+    rc, ctx = _create(N.IMPLICIT_EULER, 32, neq=64, npar=65)
+    assert rc == N.OK
+    assert "#define SODECL_HAS_ROW_BAND 1" in N.program_source(ctx)
+    N.lib.sodecl_cuda_destroy(ctx)
+    rc, ctx = _create(N.IMPLICIT_EULER, 32, neq=64, npar=65, drop="sode_system_row_band")
+    assert rc == N.OK  # an accelerator only: the lanes still run without it
+    assert "#define SODECL_HAS_ROW_BAND 0" in N.program_source(ctx)
     N.lib.sodecl_cuda_destroy(ctx)
