@@ -48,6 +48,13 @@ OPC_CMP(<) OPC_CMP(>) OPC_CMP(<=) OPC_CMP(>=) OPC_CMP(==) OPC_CMP(!=)
     inline Counted name(Counted a) { ++Counted::fun; return Counted(std::name(a.v)); }
 OPC_FUN(exp) OPC_FUN(log) OPC_FUN(sin) OPC_FUN(cos) OPC_FUN(sqrt) OPC_FUN(tanh) OPC_FUN(tan)
 inline Counted fabs(Counted a) { return Counted(std::fabs(a.v)); }
+// OpenCL C's sincos(x, &c): two math calls
+inline Counted sincos(Counted a, Counted *c)
+{
+    Counted::fun += 2;
+    *c = Counted(std::cos(a.v));
+    return Counted(std::sin(a.v));
+}
 inline Counted pow(Counted a, Counted b) { ++Counted::fun; return Counted(std::pow(a.v, b.v)); }
 using std::exp; using std::log; using std::sin; using std::cos; using std::sqrt; using std::fabs;
 

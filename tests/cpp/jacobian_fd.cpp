@@ -7,6 +7,13 @@
 #include <cmath>
 #include <cstdio>
 
+// OpenCL C's sincos(x, &c): returns sin(x), stores cos(x)
+static double sincos(double x, double *c)
+{
+    *c = std::cos(x);
+    return std::sin(x);
+}
+
 #define _numeq_ NUMEQ
 #define _numpar_ NUMPAR
 #define _numnoi_ 1
