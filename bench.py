@@ -273,7 +273,7 @@ def main():
                 "hbm_frac_of_measured": (hbm_gbs / hbm_peak) if hbm_peak else None,
                 "peak_source": "measured on this GPU: FMA-chain microbenchmark (sodecl_cuda_fma_peak), 2 flops/FMA",
                 "ops_per_orbit_step": RK4_OPS_PER_ORBIT_STEP,
-                "fp64_pipe_active": "59.5 % of peak (ncu sm__pipe_fp64_cycles_active, 2^18-orbit x 1000-step "
+                "fp64_pipe_active": "59.1 % of peak (ncu sm__pipe_fp64_cycles_active, 2^18-orbit x 1000-step "
                                     "launch of this kernel); counted source ops understate the pipe work, exp and "
                                     "division expanding to many FP64 instructions each"}
 

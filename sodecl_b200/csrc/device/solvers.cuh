@@ -431,9 +431,10 @@ __device__ __forceinline__ double sodecl_counter_plus(double counter, int c)
 }
 
 #if SODECL_SOLVER == 3 || SODECL_SOLVER == 4
-// sodecl_band_solve on the shared band system (D, UP, LO, V) -> DX, by one lane.
-// (Plain quotients: with the loop rolled, sharing each pivot's reciprocal
-// between the two sweeps was measured slower here.)
+// sodecl_band_solve on the shared band system (D, UP, LO, V), in two parts: the
+// forward sweep, a recurrence through the pivots, by one lane (IEEE quotients
+// on the recurrence's chain: a reciprocal there was measured slower), and
+// sodecl_lanes_back_subst -> DX.
 __device__ __forceinline__ void sodecl_lanes_band_solve(const sodecl_lanes_view &v)
 {
     real_t dprev = v.D[0], vprev = v.V[0];
@@ -447,12 +448,29 @@ __device__ __forceinline__ void sodecl_lanes_band_solve(const sodecl_lanes_view 
         v.D[i] = dprev;
         v.V[i] = vprev;
     }
-    real_t x = sodecl_qdiv(v.V[_numeq_ - 1], v.D[_numeq_ - 1]);
-    v.DX[_numeq_ - 1] = x;
+}
+
+// The back substitution, after the forward sweep: every lane of the group
+// takes the reciprocals of its rows' pivots at once (into UP, which only the
+// forward sweep reads), then the first lane finishes each quotient from them
+// (sodecl_pdiv: the IEEE quotient's bits; a plain quotient in other builds),
+// which shortens its dependent chain.  Called by every lane of the group.
+__device__ __forceinline__ void sodecl_lanes_back_subst(const sodecl_lanes_view &v)
+{
+#pragma unroll
+    for (int k = 0; k < SODECL_ROWS; ++k) {
+        const int row = v.lane + k * SODECL_LANES;
+        if (row < _numeq_) v.UP[row] = sodecl_pivot_rcp(v.D[row]);
+    }
+    __syncwarp(v.mask);
+    if (v.lane == 0) {
+        real_t x = sodecl_qdiv(v.V[_numeq_ - 1], v.D[_numeq_ - 1]);
+        v.DX[_numeq_ - 1] = x;
 #pragma unroll 1
-    for (int i = _numeq_ - 2; i >= 0; --i) {
-        x = sodecl_qdiv(v.V[i] - v.LO[i] * x, v.D[i]);
-        v.DX[i] = x;
+        for (int i = _numeq_ - 2; i >= 0; --i) {
+            x = sodecl_pdiv(v.V[i] - v.LO[i] * x, v.D[i], v.UP[i]);
+            v.DX[i] = x;
+        }
     }
 }
 
@@ -542,6 +560,8 @@ __device__ __forceinline__ int sodecl_lanes_newton(real_t h, real_t t, const rea
         }
         __syncwarp(v.mask);
         if (v.lane == 0) sodecl_lanes_band_solve(v);
+        __syncwarp(v.mask);
+        sodecl_lanes_back_subst(v);
         __syncwarp(v.mask);
 #pragma unroll
         for (int k = 0; k < SODECL_ROWS; ++k) {

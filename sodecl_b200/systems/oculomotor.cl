@@ -38,11 +38,14 @@
  * written with one exp whose argument is selected: x / (-bt) rounds exactly
  * as (-x) / bt, so each branch's value is the same to the last bit, and the
  * orbits of a warp on either side of x = 0 share one exp instead of running
- * both branches one after the other */
+ * both branches one after the other.  The argument selects between two
+ * quotients, not between two divisors: bt and b are fixed for an orbit, so
+ * where the compiler computes quotients through reciprocals it takes both
+ * reciprocals once, outside the step loop */
 double ocm_burst(double x, double a, double b, double at, double bt)
 {
 	int right = x > 0;
-	double e = exp(x / (right ? -bt : b));
+	double e = exp(right ? x / -bt : x / b);
 	return right ? (at * (1.00 - e)) : (-(a / b) * x * e);
 }
 
