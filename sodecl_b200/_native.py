@@ -147,8 +147,6 @@ SIGNATURES = {
                                            C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sodecl_cuda_division_check": (C.c_int, [C.c_int, C.c_int64, C.c_uint64, C.POINTER(C.c_int64),
                                              C.POINTER(C.c_double), C.POINTER(C.c_double)]),
-    "sodecl_cuda_division_check_f32": (C.c_int, [C.c_int, C.c_int64, C.c_uint64, C.POINTER(C.c_int64),
-                                                 C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "sodecl_class_cfg_init": (None, [C.POINTER(ClassCfg)]),
     "sodecl_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(_P)]),
     "sodecl_batch_add_class": (C.c_int, [_P, C.c_char_p, C.c_size_t, C.POINTER(ClassCfg), C.POINTER(C.c_int32)]),

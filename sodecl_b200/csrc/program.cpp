@@ -420,8 +420,8 @@ std::string assemble(const ProgramSpec &spec, const std::string &system_src, con
     if (spec.fp32) eps = suffix_in_code(eps);
     s << "#define _epsilon1_ " << eps << "\n";
     s << l2_bound_define(spec.newton_tol, spec.fp32);
-    if (spec.fast_div) s << "#define double sodecl_num\n";
-    else if (spec.fp32) s << "#define double float\n";
+    if (spec.fp32) s << "#define double float\n";
+    else if (spec.fast_div) s << "#define double sodecl_f64\n";
     s << "#line 1 \"system.cl\"\n";
     const std::string user = relax_parameter_bounds(system_src);
     s << (spec.fp32 ? suffix_float_literals(user) : user) << "\n";
@@ -559,7 +559,7 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
         s << "#define _epsilon1_ " << print_like_reference(sp.newton_tol) << "\n";
         s << l2_bound_define(sp.newton_tol, false);
         s << "namespace sodecl_cls_" << k << " {\n";
-        if (fast_div) s << "#define double sodecl_num\n";
+        if (fast_div) s << "#define double sodecl_f64\n";
         s << "#line 1 \"class" << k << ".cl\"\n" << relax_parameter_bounds(src) << "\n";
         if (fast_div) s << "#undef double\n";
         for (const auto &m : defined_macros(src)) s << "#undef " << m << "\n";
@@ -611,7 +611,7 @@ std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, in
     s << l2_bound_define(spec.newton_tol, false);
     const std::string user = relax_parameter_bounds(src);
     const std::vector<std::string> macros = defined_macros(src);
-    if (fast_div) s << "#define double sodecl_num\n";
+    if (fast_div) s << "#define double sodecl_f64\n";
     s << "#line 1 \"system.cl\"\n" << user << "\n";
     if (fast_div) s << "#undef double\n";
     for (const auto &m : macros) s << "#undef " << m << "\n";
@@ -661,6 +661,7 @@ std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string 
 {
     const SystemTraits traits = inspect_system(system_src);
     ProgramSpec s = spec;
+    if (s.fp32) s.fast_div = false;
     // the wrapper type would hand a struct to printf's varargs
     if (s.fast_div && system_src.find("printf") != std::string::npos) s.fast_div = false;
     if (!s.fast_div) return compile_one(s, system_src, traits);

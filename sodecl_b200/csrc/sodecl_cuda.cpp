@@ -719,14 +719,16 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
     };
     std::vector<Cand> cands = {{128, 0, SODECL_DIV_IEEE, 1}, {128, 4, SODECL_DIV_IEEE, 1},
                                {256, 3, SODECL_DIV_IEEE, 1}, {64, 0, SODECL_DIV_IEEE, 1}};
-    cands.push_back({128, 0, SODECL_DIV_RECIPROCAL, 1});
-    cands.push_back({128, 4, SODECL_DIV_RECIPROCAL, 1});
+    if (ctx->cfg.precision == SODECL_FP64) {
+        cands.push_back({128, 0, SODECL_DIV_RECIPROCAL, 1});
+        cands.push_back({128, 4, SODECL_DIV_RECIPROCAL, 1});
+    }
     // lanes per orbit: up to the first power of two >= the equations
     const auto traits = sodecl_b200::inspect_system(ctx->system_src);
     const int solver = ctx->cfg.solver;
     // implicit solvers run under a register cap by default (min_blocks 0); 1 lifts it
     if (solver == SODECL_IMPLICIT_EULER || solver == SODECL_IMPLICIT_MIDPOINT)
-        cands.push_back({128, 1, SODECL_DIV_RECIPROCAL, 1});
+        cands.push_back({128, 1, ctx->cfg.precision == SODECL_FP64 ? SODECL_DIV_RECIPROCAL : SODECL_DIV_IEEE, 1});
     const bool row_ok = lanes_supported(traits, solver);
     if (row_ok) {
         for (int l = 2; l <= 32 && l / 2 < ctx->cfg.num_equat; l *= 2) {
