@@ -722,6 +722,7 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
     if (ctx->cfg.precision == SODECL_FP64) {
         cands.push_back({128, 0, SODECL_DIV_RECIPROCAL, 1});
         cands.push_back({128, 4, SODECL_DIV_RECIPROCAL, 1});
+        cands.push_back({128, 3, SODECL_DIV_RECIPROCAL, 1});
     }
     // lanes per orbit: up to the first power of two >= the equations
     const auto traits = sodecl_b200::inspect_system(ctx->system_src);
