@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SODECL_CUDA_ABI_VERSION 2
+#define SODECL_CUDA_ABI_VERSION 3
 
 /* status codes */
 #define SODECL_OK 0
@@ -54,6 +54,12 @@ extern "C" {
 #define SODECL_RUNGE_KUTTA 2
 #define SODECL_IMPLICIT_EULER 3
 #define SODECL_IMPLICIT_MIDPOINT 4
+/* No counterpart in the reference (its README lists variable-step solvers as
+ * future work): Dormand-Prince 5(4) with adaptive steps per orbit.  Records
+ * land on the same grid as the fixed-step solvers (every kernel_steps * dt);
+ * dt is the first step tried; rtol, atol and max_steps below control it.
+ * One thread per orbit; not in batches or the adjoint. */
+#define SODECL_DORMAND_PRINCE 5
 
 #define SODECL_FP64 0
 #define SODECL_FP32 1
@@ -69,7 +75,9 @@ extern "C" {
 #define SODECL_DIV_IEEE 1
 
 /* per-orbit status flags (sodecl_cuda_status) */
-#define SODECL_FLAG_NEWTON_CAP 1   /* some implicit step stopped at newton_max_iter */
+#define SODECL_FLAG_NEWTON_CAP 1   /* some implicit step stopped at newton_max_iter, or an
+                                      adaptive record interval ran out of max_steps or of
+                                      representable step sizes (its state is then NaN) */
 #define SODECL_FLAG_NONFINITE 2    /* a stored record held NaN or Inf */
 
 typedef struct sodecl_ctx sodecl_ctx;
@@ -77,7 +85,7 @@ typedef struct sodecl_ctx sodecl_ctx;
 /* Run configuration: the reference's constructor arguments
  * (include/sodeclmgr.hpp:122-124) plus this library's options. */
 typedef struct sodecl_cfg {
-    int32_t solver;          /* SODECL_STOCHASTIC_EULER .. SODECL_IMPLICIT_MIDPOINT */
+    int32_t solver;          /* SODECL_STOCHASTIC_EULER .. SODECL_DORMAND_PRINCE */
     double dt;               /* step; the program steps with dt printed to 6 significant
                                 digits, as the reference's #define _m_dt_ does */
     double int_time;         /* tspan: records = count(j < int_time/(dt*kernel_steps)) + 1 */
@@ -104,10 +112,14 @@ typedef struct sodecl_cfg {
                                 file's sode_system_row (and sode_system_stoch_row for the
                                 stochastic solver); Euler, RK4 and Euler-Maruyama only.
                                 Same results either way.  No counterpart in the reference. */
+    double rtol;             /* SODECL_DORMAND_PRINCE: relative and absolute error per step, */
+    double atol;             /*   err_i / (atol + rtol max(|y_i|, |y5_i|)) in RMS <= 1; default 1e-6, 1e-9 */
+    int32_t max_steps;       /* SODECL_DORMAND_PRINCE: step attempts per record interval; default 100000 */
 } sodecl_cfg;
 
 /* Fills the defaults: Euler, fp64, fmad on, Newton 1e-7 / 1000, device 0,
- * reciprocal division, one thread per orbit. */
+ * reciprocal division, one thread per orbit, rtol 1e-6, atol 1e-9, 100000
+ * adaptive steps per record interval. */
 void sodecl_cfg_init(sodecl_cfg *cfg);
 
 /* Validates cfg and makes a context bound to cfg->device.  Needs no GPU
@@ -125,6 +137,9 @@ int sodecl_cuda_compile(sodecl_ctx *ctx, const char *system_src, size_t len);
  * params[list_size][num_params] (orbit-major, as the reference's host arrays),
  * counters[list_size] the noise draw counters (stochastic solver; NULL draws
  * them as the reference does, U(-1e11, 1e11), from a generator seeded with 0).
+ * For SODECL_DORMAND_PRINCE the same array holds each orbit's next step size
+ * (NULL or values <= 0: start with dt), kept across runs and launches so that
+ * results do not depend on how a run is split.
  * Replaces set_t0/set_y0/set_params + create_buffers/write_buffers
  * (src/sodeclmgr.cpp:654-829, counters :48-59). */
 int sodecl_cuda_upload(sodecl_ctx *ctx, const double *t0, const double *y0, const double *params,
@@ -145,8 +160,8 @@ int sodecl_cuda_run(sodecl_ctx *ctx, double *out, int64_t out_len);
 /* Copies the current state back: any pointer may be NULL. */
 int sodecl_cuda_download_state(sodecl_ctx *ctx, double *t, double *y, double *counters);
 
-/* Per-orbit status accumulated since upload: Newton passes taken and
- * SODECL_FLAG_* bits.  Either pointer may be NULL.  (No counterpart in the
+/* Per-orbit status accumulated since upload: Newton passes taken (accepted
+ * steps for SODECL_DORMAND_PRINCE) and SODECL_FLAG_* bits.  Either pointer may be NULL.  (No counterpart in the
  * reference, which reports nothing per orbit.) */
 int sodecl_cuda_status(sodecl_ctx *ctx, int64_t *newton_passes, int32_t *flags);
 
@@ -173,7 +188,8 @@ int sodecl_cuda_device_count(int *count);
 /* One launch over caller-owned device buffers, on the caller's stream
  * (NULL = the legacy default stream).  Pointers are device pointers:
  * t[n], y[n][neq], params[n][npar] (doubles, in/out except params),
- * counters[n] (stochastic solver), records = base of a window
+ * counters[n] (stochastic solver; step sizes for SODECL_DORMAND_PRINCE,
+ * nullable there), records = base of a window
  * [record][neq][rec_stride] of double (or float with cfg.record_f32) whose
  * first row is record rec_first.  Runs record intervals
  * [chunk_begin, chunk_end), storing each interval's starting state, and the

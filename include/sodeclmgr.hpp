@@ -18,7 +18,10 @@
 namespace sodecl {
 
 // include/solver_Type.hpp:14-20 of the reference
-enum class solver_Type { StochasticEuler = 0, Euler = 1, RungeKutta = 2, ImplicitEuler = 3, ImplicitMidpoint = 4 };
+// DormandPrince (adaptive steps) has no counterpart in the reference
+enum class solver_Type {
+    StochasticEuler = 0, Euler = 1, RungeKutta = 2, ImplicitEuler = 3, ImplicitMidpoint = 4, DormandPrince = 5
+};
 
 // include/output_Type.hpp:14-18 of the reference
 enum class output_Type { None = 0, Array = 1, File = 2 };
@@ -65,6 +68,7 @@ class sodeclmgr {
     // without them the counters are drawn as the reference draws them.
     void set_noise_counters(const double *counters);
     void set_newton(double tol, int max_iter);
+    void set_tolerances(double rtol, double atol, int max_steps);  // solver_Type::DormandPrince
     void set_precision(int precision);  // SODECL_FP64 or SODECL_FP32
     void set_fmad(bool on);
     sodecl_ctx *context() const { return m_ctx; }

@@ -105,7 +105,9 @@ def _compile(source: str, target: str, extra: list[str]) -> str:
     os.makedirs(os.path.dirname(target), exist_ok=True)
     flags = CFLAGS if "-ffp-contract=fast" not in extra else [f for f in CFLAGS if f != "-ffp-contract=off"]
     cmd = ["gcc"] + flags + ["-I", HERE] + extra + ["-x", "c", "-", "-o", target, "-lm"]
-    digest = hashlib.sha256((" ".join(cmd) + "\0" + source).encode()).hexdigest()
+    # the unit only names the headers it includes: their text goes into the digest too
+    headers = "".join(open(os.path.join(HERE, h)).read() for h in sorted(os.listdir(HERE)) if h.endswith(".h"))
+    digest = hashlib.sha256((" ".join(cmd) + "\0" + source + "\0" + headers).encode()).hexdigest()
     if _stamp_ok(target, digest):
         return target
     proc = subprocess.run(cmd, input=source.encode(), capture_output=True)

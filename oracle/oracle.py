@@ -52,7 +52,7 @@ class _Job(C.Structure):
                 ("orbit_offset", C.c_long), ("t", C.c_void_p), ("y", C.c_void_p), ("p", C.c_void_p),
                 ("counters", C.c_void_p), ("records", C.c_void_p), ("newton_tol", C.c_double),
                 ("newton_max_iter", C.c_int), ("newton_passes", C.c_void_p), ("flags", C.c_void_p),
-                ("nthreads", C.c_int)]
+                ("nthreads", C.c_int), ("rtol", C.c_double), ("atol", C.c_double), ("max_steps", C.c_int)]
 
 
 class _RefJob(C.Structure):
@@ -103,9 +103,12 @@ class Oracle:
 
     def run(self, solver, t0, y0, params, *, neq, npar, nnoi=0, dt, tspan=None, ksteps,
             nchunks=None, counters=None, orbit_offset=0, newton_tol=NEWTON_TOL_DEFAULT,
-            newton_max_iter=NEWTON_MAX_DEFAULT, records=True, nthreads=0) -> Result:
+            newton_max_iter=NEWTON_MAX_DEFAULT, records=True, nthreads=0, rtol=1e-6, atol=1e-9,
+            max_steps=100000) -> Result:
         """Integrate like the reference's run loop.  ``dt`` is the user's step;
-        the solver steps with ``printed_dt(dt)``."""
+        the solver steps with ``printed_dt(dt)``.  Solver 5 (Dormand-Prince,
+        adaptive; no reference counterpart) takes ``printed_dt(dt)`` as its
+        first step and ``counters`` as the orbits' step sizes (in/out)."""
         if nchunks is None:
             nchunks = num_chunks(tspan, dt, ksteps)
         t = _f64(t0)
@@ -118,7 +121,7 @@ class Oracle:
         flags = np.zeros(n, dtype=np.int32)
         job = _Job(solver, neq, npar, nnoi, ksteps, printed_dt(dt), nchunks, n, orbit_offset,
                    _ptr(t), _ptr(y), _ptr(p), _ptr(cnt), _ptr(rec), newton_tol, newton_max_iter,
-                   _ptr(passes), _ptr(flags), nthreads)
+                   _ptr(passes), _ptr(flags), nthreads, rtol, atol, max_steps)
         rc = self.lib.oracle_run(C.byref(job))
         if rc != 0:
             raise RuntimeError("oracle_run failed with %d" % rc)

@@ -41,7 +41,8 @@ long g_sodecl_listsize;
 double g_sodecl_dt;
 double g_sodecl_eps;
 
-enum { ORC_STOCH_EULER = 0, ORC_EULER = 1, ORC_RK4 = 2, ORC_IMPLICIT_EULER = 3, ORC_IMPLICIT_MIDPOINT = 4 };
+enum { ORC_STOCH_EULER = 0, ORC_EULER = 1, ORC_RK4 = 2, ORC_IMPLICIT_EULER = 3, ORC_IMPLICIT_MIDPOINT = 4,
+       ORC_DORMAND_PRINCE = 5 };
 enum { ORC_FLAG_NEWTON_CAP = 1, ORC_FLAG_NONFINITE = 2 };
 
 /* ---------------------------------------------------------------------- */
@@ -160,6 +161,95 @@ static int orc_implicit_midpoint(orc_real h, orc_real t, orc_real *y, orc_real *
 #endif
 
 /* ---------------------------------------------------------------------- */
+/* Dormand-Prince 5(4) with adaptive steps over one record interval [t, t +
+ * span] (Dormand & Prince, J. Comput. Appl. Math. 6(1), 1980; step control as
+ * in Hairer, Norsett & Wanner, Solving ODEs I, II.4).  The reference has no
+ * variable-step solver; this restates the library's own, in the same order
+ * of operations: RMS error over equations of e_i / (atol + rtol max(|y_i|,
+ * |y5_i|)) accepted at <= 1, next step hh * min(5, max(0.2, 0.9 err^-0.2)),
+ * not larger after a rejection, the proposal kept when the step was cut to
+ * the interval's end; first stage re-evaluated at each interval's start.
+ * Returns 0 (state NaN) when the interval needs more than max_steps attempts
+ * or a step too small to advance t.                                        */
+static int orc_dp_interval(orc_real *t_io, orc_real *y, orc_real *p, orc_real *h_io, orc_real span, double rtol,
+                           double atol, int max_steps, long *accepted)
+{
+    const int n = g_sodecl_numeq;
+    orc_real k1[n], k2[n], k3[n], k4[n], k5[n], k6[n], k7[n], yt[n], y5[n];
+    orc_real t = *t_io, h = *h_io;
+    const orc_real t_end = t + span;
+    int finite = 1;
+    for (int e = 0; e < n; ++e) finite = finite && isfinite(y[e]);
+    if (!finite) {
+        *t_io = t_end;
+        return 1;
+    }
+    if (!(h > 0) || !isfinite(h)) h = (orc_real)g_sodecl_dt;
+    sode_system(t, y, k1, p);
+    int rejected = 0;
+    for (int it = 0; t < t_end; ++it) {
+        if (it >= max_steps) break;
+        const int last = t + h >= t_end;
+        const orc_real hh = last ? t_end - t : h;
+        if (!(hh > 0) || t + hh == t) break;
+        for (int e = 0; e < n; ++e) yt[e] = y[e] + hh * (ORC_C(1.0 / 5.0) * k1[e]);
+        sode_system(t + ORC_C(1.0 / 5.0) * hh, yt, k2, p);
+        for (int e = 0; e < n; ++e) yt[e] = y[e] + hh * (ORC_C(3.0 / 40.0) * k1[e] + ORC_C(9.0 / 40.0) * k2[e]);
+        sode_system(t + ORC_C(3.0 / 10.0) * hh, yt, k3, p);
+        for (int e = 0; e < n; ++e)
+            yt[e] = y[e] + hh * (ORC_C(44.0 / 45.0) * k1[e] + ORC_C(-56.0 / 15.0) * k2[e] + ORC_C(32.0 / 9.0) * k3[e]);
+        sode_system(t + ORC_C(4.0 / 5.0) * hh, yt, k4, p);
+        for (int e = 0; e < n; ++e)
+            yt[e] = y[e] + hh * (ORC_C(19372.0 / 6561.0) * k1[e] + ORC_C(-25360.0 / 2187.0) * k2[e] +
+                                 ORC_C(64448.0 / 6561.0) * k3[e] + ORC_C(-212.0 / 729.0) * k4[e]);
+        sode_system(t + ORC_C(8.0 / 9.0) * hh, yt, k5, p);
+        for (int e = 0; e < n; ++e)
+            yt[e] = y[e] + hh * (ORC_C(9017.0 / 3168.0) * k1[e] + ORC_C(-355.0 / 33.0) * k2[e] +
+                                 ORC_C(46732.0 / 5247.0) * k3[e] + ORC_C(49.0 / 176.0) * k4[e] +
+                                 ORC_C(-5103.0 / 18656.0) * k5[e]);
+        sode_system(t + hh, yt, k6, p);
+        for (int e = 0; e < n; ++e)
+            y5[e] = y[e] + hh * (ORC_C(35.0 / 384.0) * k1[e] + ORC_C(500.0 / 1113.0) * k3[e] +
+                                 ORC_C(125.0 / 192.0) * k4[e] + ORC_C(-2187.0 / 6784.0) * k5[e] +
+                                 ORC_C(11.0 / 84.0) * k6[e]);
+        sode_system(t + hh, y5, k7, p);
+        orc_real acc = 0;
+        for (int e = 0; e < n; ++e) {
+            const orc_real err = hh * (ORC_C(71.0 / 57600.0) * k1[e] + ORC_C(-71.0 / 16695.0) * k3[e] +
+                                       ORC_C(71.0 / 1920.0) * k4[e] + ORC_C(-17253.0 / 339200.0) * k5[e] +
+                                       ORC_C(22.0 / 525.0) * k6[e] + ORC_C(-1.0 / 40.0) * k7[e]);
+            const orc_real sc = ORC_C(atol) + ORC_C(rtol) * fmax(fabs(y[e]), fabs(y5[e]));
+            const orc_real q = err / sc;
+            acc = acc + q * q;
+        }
+        const orc_real err = sqrt(acc / (orc_real)n);
+        orc_real fac = (err > 0) ? ORC_C(0.9) * exp(ORC_C(-0.2) * log(err)) : ORC_C(5.0);
+        fac = fmin(ORC_C(5.0), fmax(ORC_C(0.2), fac));
+        if (err <= 1) {
+            t = last ? t_end : t + hh;
+            for (int e = 0; e < n; ++e) {
+                y[e] = y5[e];
+                k1[e] = k7[e];
+            }
+            ++*accepted;
+            if (!last) h = hh * (rejected ? fmin((orc_real)1, fac) : fac);
+            rejected = 0;
+        } else {
+            h = hh * (err == err ? fmin((orc_real)1, fac) : ORC_C(0.2));
+            rejected = 1;
+        }
+    }
+    *h_io = h;
+    if (t < t_end) {
+        for (int e = 0; e < n; ++e) y[e] = (orc_real)NAN;
+        *t_io = t_end;
+        return 0;
+    }
+    *t_io = t;
+    return 1;
+}
+
+/* ---------------------------------------------------------------------- */
 /* Threefry-2x64 with 20 rounds (Salmon, Moraes, Dror, Shaw, "Parallel random
  * numbers: as easy as 1, 2, 3", SC'11): the Threefish-derived block cipher
  * with rotation schedule 16,42,12,31,16,32,24,21, key-schedule parity word
@@ -269,6 +359,8 @@ typedef struct oracle_job {
     long *newton_passes;     /* [n] or NULL */
     int *flags;              /* [n] or NULL */
     int nthreads;            /* 0: OpenMP default */
+    double rtol, atol;       /* solver 5: error tolerances */
+    int max_steps;           /* solver 5: step attempts per record interval */
 } oracle_job;
 
 /* Runs every orbit of the job: the record before each interval of ksteps
@@ -290,7 +382,7 @@ int oracle_run(const oracle_job *job)
         return -6;
 #endif
     }
-    if (job->solver < 0 || job->solver > 4) return -1;
+    if (job->solver < 0 || job->solver > 5) return -1;
 
     g_sodecl_numeq = job->neq;
     g_sodecl_numpar = job->npar;
@@ -319,11 +411,20 @@ int oracle_run(const oracle_job *job)
         int capped = 0;
         (void)noise; (void)sqrt_h; (void)capped;
 
+        /* solver 5: the orbit's next step size rides in the counters array */
+        orc_real hstate = (orc_real)counter;
+        const orc_real span = (orc_real)job->ksteps * h;
         for (long c = 0; c <= job->nchunks; ++c) {
             if (job->records)
                 for (int e = 0; e < neq; ++e)
                     job->records[((size_t)c * neq + e) * n + i] = (double)y[e];
             if (c == job->nchunks) break;
+            if (job->solver == ORC_DORMAND_PRINCE) {
+                if (!orc_dp_interval(&t, y, p, &hstate, span, job->rtol, job->atol, job->max_steps, &passes))
+                    capped = 1;
+                counter = (double)hstate;
+                continue;
+            }
             for (int s = 0; s < job->ksteps; ++s) {
                 switch (job->solver) {
                 case ORC_EULER: orc_euler(h, t, y, ynew, p); break;

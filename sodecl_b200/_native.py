@@ -22,7 +22,9 @@ ERR_NO_STOCH = -7
 ERR_OUT_OF_MEMORY = -8
 ERR_UNSUPPORTED = -9
 
-STOCHASTIC_EULER, EULER, RUNGE_KUTTA, IMPLICIT_EULER, IMPLICIT_MIDPOINT = range(5)
+# include/sodecl_cuda.h's SODECL_CUDA_ABI_VERSION, which the structures below follow
+ABI_VERSION = 3
+STOCHASTIC_EULER, EULER, RUNGE_KUTTA, IMPLICIT_EULER, IMPLICIT_MIDPOINT, DORMAND_PRINCE = range(6)
 FP64, FP32 = 0, 1
 DIV_RECIPROCAL, DIV_IEEE = 0, 1
 FLAG_NEWTON_CAP = 1
@@ -49,6 +51,9 @@ class Cfg(C.Structure):
         ("min_blocks_per_sm", C.c_int32),
         ("division", C.c_int32),
         ("lanes_per_orbit", C.c_int32),
+        ("rtol", C.c_double),
+        ("atol", C.c_double),
+        ("max_steps", C.c_int32),
     ]
 
 
@@ -176,6 +181,9 @@ def _load():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
+    if lib.sodecl_cuda_abi_version() != ABI_VERSION:
+        raise ImportError("%s has ABI version %d, these bindings %d: rebuild it" %
+                          (LIB_PATH, lib.sodecl_cuda_abi_version(), ABI_VERSION))
     return lib
 
 

@@ -19,7 +19,8 @@ from . import _native as N
 
 SOLVERS = {"se": N.STOCHASTIC_EULER, "stochastic_euler": N.STOCHASTIC_EULER, "euler": N.EULER, "e": N.EULER,
            "rk4": N.RUNGE_KUTTA, "r": N.RUNGE_KUTTA, "runge_kutta": N.RUNGE_KUTTA, "ie": N.IMPLICIT_EULER,
-           "implicit_euler": N.IMPLICIT_EULER, "im": N.IMPLICIT_MIDPOINT, "implicit_midpoint": N.IMPLICIT_MIDPOINT}
+           "implicit_euler": N.IMPLICIT_EULER, "im": N.IMPLICIT_MIDPOINT, "implicit_midpoint": N.IMPLICIT_MIDPOINT,
+           "dp45": N.DORMAND_PRINCE, "dopri5": N.DORMAND_PRINCE, "dormand_prince": N.DORMAND_PRINCE}
 SYSTEMS_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "systems")
 
 
@@ -49,7 +50,8 @@ class Integrator:
 
     def __init__(self, system, solver, *, dt, tspan, ksteps, neq, npar, orbits, nnoi=0, device=0,
                  precision="fp64", fmad=True, newton_tol=1e-7, newton_max_iter=1000, block=0,
-                 record_f32=False, min_blocks=0, division="reciprocal", lanes=1, system_src=None):
+                 record_f32=False, min_blocks=0, division="reciprocal", lanes=1, system_src=None, rtol=1e-6,
+                 atol=1e-9, max_steps=100000):
         cfg = N.Cfg()
         N.lib.sodecl_cfg_init(C.byref(cfg))
         cfg.solver = _solver_id(solver)
@@ -70,6 +72,9 @@ class Integrator:
         cfg.min_blocks_per_sm = int(min_blocks)
         cfg.division = N.DIV_RECIPROCAL if str(division).lower() == "reciprocal" else N.DIV_IEEE
         cfg.lanes_per_orbit = int(lanes)
+        cfg.rtol = float(rtol)
+        cfg.atol = float(atol)
+        cfg.max_steps = int(max_steps)
         self.cfg = cfg
         self._ctx = C.c_void_p()
         rc = N.lib.sodecl_cuda_create(C.byref(cfg), C.byref(self._ctx))

@@ -306,6 +306,118 @@ __device__ __forceinline__ void sodecl_step_em(real_t h, real_t t, real_t *y, re
 }
 #endif
 
+#if SODECL_SOLVER == 5
+#if SODECL_LANES > 1 || defined(SODECL_STEPS_ONLY)
+#error "the adaptive solver runs one thread per orbit, in single-system programs"
+#endif
+// Dormand-Prince 5(4) with adaptive steps (J. R. Dormand, P. J. Prince, "A
+// family of embedded Runge-Kutta formulae", J. Comput. Appl. Math. 6(1), 1980;
+// step control as in Hairer, Norsett, Wanner, "Solving Ordinary Differential
+// Equations I", II.4).  No counterpart in the reference, which lists
+// variable-step solvers as future work.
+//
+// sodecl_dp_interval integrates the orbit from t to t + span (one record
+// interval), the last step cut to land on it exactly.  A step of size hh is
+// accepted when the RMS over equations of e_i / (atol + rtol max(|y_i|, |y5_i|))
+// is at most 1 (e the difference of the embedded 5th- and 4th-order results);
+// the next step is hh * min(5, max(0.2, 0.9 err^(-1/5))), not larger than hh
+// after a rejection; a step cut to the interval's end leaves the proposal `h`
+// as it was.  The first stage is re-evaluated at each interval's start, so
+// results do not depend on how intervals are grouped into launches.  Returns
+// false (state NaN) when the interval needs more than SODECL_MAX_STEPS
+// attempts or a step too small to advance t.
+#define SODECL_DP(c) ((real_t)(c))
+__device__ __forceinline__ bool sodecl_dp_interval(real_t &t, real_t *y, real_t *p, real_t &h, const real_t span,
+                                                   sodecl_i64 &accepted)
+{
+    real_t k1[_numeq_], k2[_numeq_], k3[_numeq_], k4[_numeq_], k5[_numeq_], k6[_numeq_], k7[_numeq_];
+    real_t yt[_numeq_], y5[_numeq_];
+    const real_t t_end = t + span;
+    bool finite = true;
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) finite = finite && isfinite(y[e]);
+    if (!finite) {  // a diverged orbit stays as it is
+        t = t_end;
+        return true;
+    }
+    if (!(h > (real_t)0) || !isfinite(h)) h = (real_t)_m_dt_;
+    sode_system(t, y, k1, p);
+    bool rejected = false;
+#pragma unroll 1
+    for (int n = 0; t < t_end; ++n) {
+        if (n >= SODECL_MAX_STEPS) break;
+        const bool last = t + h >= t_end;
+        const real_t hh = last ? t_end - t : h;
+        if (!(hh > (real_t)0) || t + hh == t) break;
+#pragma unroll SODECL_EQ_UNROLL
+        for (int e = 0; e < _numeq_; ++e) yt[e] = y[e] + hh * (SODECL_DP(1.0 / 5.0) * k1[e]);
+        sode_system(t + SODECL_DP(1.0 / 5.0) * hh, yt, k2, p);
+#pragma unroll SODECL_EQ_UNROLL
+        for (int e = 0; e < _numeq_; ++e)
+            yt[e] = y[e] + hh * (SODECL_DP(3.0 / 40.0) * k1[e] + SODECL_DP(9.0 / 40.0) * k2[e]);
+        sode_system(t + SODECL_DP(3.0 / 10.0) * hh, yt, k3, p);
+#pragma unroll SODECL_EQ_UNROLL
+        for (int e = 0; e < _numeq_; ++e)
+            yt[e] = y[e] + hh * (SODECL_DP(44.0 / 45.0) * k1[e] + SODECL_DP(-56.0 / 15.0) * k2[e] +
+                                 SODECL_DP(32.0 / 9.0) * k3[e]);
+        sode_system(t + SODECL_DP(4.0 / 5.0) * hh, yt, k4, p);
+#pragma unroll SODECL_EQ_UNROLL
+        for (int e = 0; e < _numeq_; ++e)
+            yt[e] = y[e] + hh * (SODECL_DP(19372.0 / 6561.0) * k1[e] + SODECL_DP(-25360.0 / 2187.0) * k2[e] +
+                                 SODECL_DP(64448.0 / 6561.0) * k3[e] + SODECL_DP(-212.0 / 729.0) * k4[e]);
+        sode_system(t + SODECL_DP(8.0 / 9.0) * hh, yt, k5, p);
+#pragma unroll SODECL_EQ_UNROLL
+        for (int e = 0; e < _numeq_; ++e)
+            yt[e] = y[e] + hh * (SODECL_DP(9017.0 / 3168.0) * k1[e] + SODECL_DP(-355.0 / 33.0) * k2[e] +
+                                 SODECL_DP(46732.0 / 5247.0) * k3[e] + SODECL_DP(49.0 / 176.0) * k4[e] +
+                                 SODECL_DP(-5103.0 / 18656.0) * k5[e]);
+        sode_system(t + hh, yt, k6, p);
+#pragma unroll SODECL_EQ_UNROLL
+        for (int e = 0; e < _numeq_; ++e)
+            y5[e] = y[e] + hh * (SODECL_DP(35.0 / 384.0) * k1[e] + SODECL_DP(500.0 / 1113.0) * k3[e] +
+                                 SODECL_DP(125.0 / 192.0) * k4[e] + SODECL_DP(-2187.0 / 6784.0) * k5[e] +
+                                 SODECL_DP(11.0 / 84.0) * k6[e]);
+        sode_system(t + hh, y5, k7, p);
+        real_t acc = 0;
+#pragma unroll SODECL_EQ_UNROLL
+        for (int e = 0; e < _numeq_; ++e) {
+            const real_t err = hh * (SODECL_DP(71.0 / 57600.0) * k1[e] + SODECL_DP(-71.0 / 16695.0) * k3[e] +
+                                     SODECL_DP(71.0 / 1920.0) * k4[e] + SODECL_DP(-17253.0 / 339200.0) * k5[e] +
+                                     SODECL_DP(22.0 / 525.0) * k6[e] + SODECL_DP(-1.0 / 40.0) * k7[e]);
+            const real_t sc = SODECL_DP(SODECL_ATOL) + SODECL_DP(SODECL_RTOL) * fmax(fabs(y[e]), fabs(y5[e]));
+            const real_t q = err / sc;
+            acc = acc + q * q;
+        }
+        const real_t err = sqrt(acc / (real_t)_numeq_);
+        real_t fac = (err > (real_t)0) ? SODECL_DP(0.9) * exp(SODECL_DP(-0.2) * log(err)) : SODECL_DP(5.0);
+        fac = fmin(SODECL_DP(5.0), fmax(SODECL_DP(0.2), fac));
+        if (err <= (real_t)1) {
+            t = last ? t_end : t + hh;
+#pragma unroll SODECL_EQ_UNROLL
+            for (int e = 0; e < _numeq_; ++e) {
+                y[e] = y5[e];
+                k1[e] = k7[e];
+            }
+            ++accepted;
+            if (!last) h = hh * (rejected ? fmin((real_t)1, fac) : fac);
+            rejected = false;
+        } else {
+            // a NaN error shrinks the step too
+            h = hh * (err == err ? fmin((real_t)1, fac) : SODECL_DP(0.2));
+            rejected = true;
+        }
+    }
+    if (t < t_end) {
+#pragma unroll SODECL_EQ_UNROLL
+        for (int e = 0; e < _numeq_; ++e) y[e] = (real_t)__longlong_as_double(0x7ff8000000000000ULL);
+        t = t_end;
+        return false;
+    }
+    return true;
+}
+#undef SODECL_DP
+#endif
+
 // One step of the configured solver from (t, y): y <- y(t + h), t <- t + h,
 // with t advanced as the reference's callers advance it
 // (solver_caller.cl:38, stochastic_solver_caller.cl:71).
@@ -708,6 +820,8 @@ __device__ __forceinline__ void sodecl_orbit_out(const sodecl_args &a, sodecl_i6
     for (int e = 0; e < _numeq_; ++e) a.y[i * _numeq_ + e] = (double)y[e];
 #if SODECL_SOLVER == 0
     a.counters[i] = counter;
+#elif SODECL_SOLVER == 5
+    if (a.counters) a.counters[i] = counter;
 #endif
     (void)counter;
     if (capped) flags |= SODECL_FLAG_NEWTON_CAP;
@@ -840,6 +954,18 @@ sodecl_orbits(const sodecl_args a)
     double counter = 0.0;
 #endif
 
+#if SODECL_SOLVER == 5
+    // the orbit's next step size rides in the counters array
+    real_t h = a.counters ? (real_t)a.counters[i] : (real_t)0;
+    const real_t span = (real_t)_numsteps_ * (real_t)_m_dt_;
+#pragma unroll 1
+    for (int c = a.chunk_begin; c < a.chunk_end; ++c) {
+        if (a.records)
+            sodecl_store_record(a, c, i, y, flags);
+        if (!sodecl_dp_interval(t, y, p, h, span, passes)) capped = 1;
+    }
+    counter = (double)h;
+#else
 #pragma unroll 1
     for (int c = a.chunk_begin; c < a.chunk_end; ++c) {
         if (a.records)
@@ -848,6 +974,7 @@ sodecl_orbits(const sodecl_args a)
         for (int s = 0; s < _numsteps_; ++s)
             sodecl_advance(t, y, p, gid, counter, passes, capped);
     }
+#endif
     sodecl_orbit_out(a, i, t, y, counter, passes, capped, flags);
 }
 #else  // SODECL_LANES > 1

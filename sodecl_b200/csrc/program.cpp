@@ -420,6 +420,11 @@ std::string assemble(const ProgramSpec &spec, const std::string &system_src, con
     if (spec.fp32) eps = suffix_in_code(eps);
     s << "#define _epsilon1_ " << eps << "\n";
     s << l2_bound_define(spec.newton_tol, spec.fp32);
+    if (spec.solver == 5) {
+        char buf[96];
+        std::snprintf(buf, sizeof buf, "#define SODECL_RTOL %a\n#define SODECL_ATOL %a\n", spec.rtol, spec.atol);
+        s << buf << "#define SODECL_MAX_STEPS " << spec.max_steps << "\n";
+    }
     if (spec.fp32) s << "#define double float\n";
     else if (spec.fast_div) s << "#define double sodecl_f64\n";
     s << "#line 1 \"system.cl\"\n";

@@ -214,7 +214,7 @@ int lanes_of(const sodecl_cfg &c) { return c.lanes_per_orbit > 1 ? c.lanes_per_o
 // with this solver.
 bool lanes_supported(const sodecl_b200::SystemTraits &t, int solver)
 {
-    if (!t.has_row) return false;
+    if (!t.has_row || solver == SODECL_DORMAND_PRINCE) return false;
     if (solver == SODECL_STOCHASTIC_EULER) return t.has_stoch_row;
     if (solver == SODECL_IMPLICIT_EULER || solver == SODECL_IMPLICIT_MIDPOINT) return t.has_jac_band;
     return true;
@@ -323,6 +323,9 @@ ProgramSpec make_spec(const sodecl_cfg &c)
         spec.min_blocks = std::max(1, 65536 / (spec.block_max * 128));
     spec.fast_div = c.division == SODECL_DIV_RECIPROCAL;
     spec.lanes = lanes_of(c);
+    spec.rtol = c.rtol;
+    spec.atol = c.atol;
+    spec.max_steps = c.max_steps;
     return spec;
 }
 
@@ -341,6 +344,9 @@ void sodecl_cfg_init(sodecl_cfg *cfg)
     cfg->newton_tol = 1e-7;
     cfg->newton_max_iter = 1000;
     cfg->division = SODECL_DIV_RECIPROCAL;
+    cfg->rtol = 1e-6;
+    cfg->atol = 1e-9;
+    cfg->max_steps = 100000;
 }
 
 int sodecl_cuda_abi_version(void) { return SODECL_CUDA_ABI_VERSION; }
@@ -381,7 +387,11 @@ int sodecl_cuda_create(const sodecl_cfg *cfg, sodecl_ctx **out)
     *out = nullptr;
     if (!cfg) return SODECL_ERR_INVALID_ARG;
     const sodecl_cfg &c = *cfg;
-    if (c.solver < 0 || c.solver > 4) return SODECL_ERR_INVALID_ARG;
+    if (c.solver < 0 || c.solver > SODECL_DORMAND_PRINCE) return SODECL_ERR_INVALID_ARG;
+    if (c.solver == SODECL_DORMAND_PRINCE &&
+        (!(c.rtol > 0) || !std::isfinite(c.rtol) || !(c.atol > 0) || !std::isfinite(c.atol) || c.max_steps < 1 ||
+         c.lanes_per_orbit > 1))
+        return SODECL_ERR_INVALID_ARG;
     if (c.num_equat < 1 || c.num_params < 0 || c.num_noi < 0 || c.list_size < 1) return SODECL_ERR_INVALID_ARG;
     if (!(c.dt > 0) || !std::isfinite(c.dt) || !(c.int_time >= 0) || !std::isfinite(c.int_time)) return SODECL_ERR_INVALID_ARG;
     if (c.kernel_steps < 1) return SODECL_ERR_INVALID_ARG;
@@ -467,7 +477,10 @@ int sodecl_cuda_upload(sodecl_ctx *ctx, const double *t0, const double *y0, cons
     if (npar > 0)
         SODECL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_p, params, n * npar * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     std::vector<double> drawn;
-    if (ctx->cfg.solver == SODECL_STOCHASTIC_EULER) {
+    if (ctx->cfg.solver == SODECL_DORMAND_PRINCE && counters) {
+        // each orbit's next step size
+        SODECL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_cnt, counters, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    } else if (ctx->cfg.solver == SODECL_STOCHASTIC_EULER) {
         const double *src = counters;
         if (!src) {
             // the reference's draw (src/sodeclmgr.cpp:48-59), seeded for reproducibility
@@ -843,8 +856,8 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     if (!ctx) return SODECL_ERR_INVALID_ARG;
     if (!io || !io->t0 || !io->y0 || (!io->params && ctx->cfg.num_params > 0) || !io->targets || !io->loss)
         return ctx->fail(SODECL_ERR_INVALID_ARG, "adjoint: t0, y0, params, targets and loss are required");
-    if (ctx->cfg.solver == SODECL_STOCHASTIC_EULER)
-        return ctx->fail(SODECL_ERR_UNSUPPORTED, "the adjoint covers the deterministic solvers");
+    if (ctx->cfg.solver == SODECL_STOCHASTIC_EULER || ctx->cfg.solver == SODECL_DORMAND_PRINCE)
+        return ctx->fail(SODECL_ERR_UNSUPPORTED, "the adjoint covers the fixed-step deterministic solvers");
     if (ctx->cfg.precision != SODECL_FP64) return ctx->fail(SODECL_ERR_UNSUPPORTED, "the adjoint is FP64");
     if (io->n < 1 || io->n > ctx->cfg.list_size) return ctx->fail(SODECL_ERR_INVALID_ARG, "adjoint: orbit count");
     if (io->tape_entries < 0 || io->tape_entries > 30000)

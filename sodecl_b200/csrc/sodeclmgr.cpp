@@ -63,6 +63,12 @@ void sodeclmgr::set_newton(double tol, int max_iter)
     m_cfg.newton_tol = tol;
     m_cfg.newton_max_iter = max_iter;
 }
+void sodeclmgr::set_tolerances(double rtol, double atol, int max_steps)
+{
+    m_cfg.rtol = rtol;
+    m_cfg.atol = atol;
+    m_cfg.max_steps = max_steps;
+}
 void sodeclmgr::set_precision(int precision) { m_cfg.precision = precision; }
 void sodeclmgr::set_fmad(bool on) { m_cfg.fmad = on ? 1 : 0; }
 

@@ -36,7 +36,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version_and_strerror():
-    assert N.lib.sodecl_cuda_abi_version() == 2
+    assert N.lib.sodecl_cuda_abi_version() == N.ABI_VERSION == 3
     assert N.lib.sodecl_cuda_strerror(N.ERR_NO_JACOBIAN).decode().startswith("implicit solver")
 
 
@@ -61,9 +61,12 @@ def test_cfg_defaults():
     N.lib.sodecl_cfg_init(C.byref(cfg))
     assert cfg.solver == N.EULER and cfg.fmad == 1 and cfg.precision == N.FP64
     assert cfg.newton_tol == 1e-7 and cfg.newton_max_iter == 1000
+    assert cfg.rtol == 1e-6 and cfg.atol == 1e-9 and cfg.max_steps == 100000
 
 
-@pytest.mark.parametrize("bad", [dict(solver=5), dict(solver=-1), dict(num_equat=0), dict(list_size=0),
+@pytest.mark.parametrize("bad", [dict(solver=6), dict(solver=-1), dict(num_equat=0), dict(list_size=0),
+                                 dict(solver=5, rtol=0.0), dict(solver=5, atol=-1.0), dict(solver=5, max_steps=0),
+                                 dict(solver=5, rtol=float("inf")), dict(solver=5, lanes_per_orbit=4),
                                  dict(dt=0.0), dict(dt=float("nan")), dict(kernel_steps=0),
                                  dict(solver=0, num_noi=0), dict(precision=2), dict(int_time=-1.0),
                                  dict(local_group_size=2048), dict(dt=1e-12, int_time=1.0, kernel_steps=1)])
@@ -85,7 +88,7 @@ def _compile(ctx, src):
     return N.lib.sodecl_cuda_compile(ctx, b, len(b))
 
 
-@pytest.mark.parametrize("solver", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("solver", [0, 1, 2, 3, 4, 5])
 @pytest.mark.parametrize("precision", [0, 1])
 def test_compile_every_solver_without_gpu(solver, precision):
     nnoi = 2 if solver == 0 else 0
