@@ -66,6 +66,27 @@ def test_oracle_step_limit_gives_nan_and_flag():
     assert np.isnan(r.records[1:]).all() and np.isfinite(r.records[0]).all()
 
 
+def test_oracle_kuramoto_and_fp32():
+    """A second system (Kuramoto N=8, non-stiff) against fine RK4, and the FP32
+    build against the FP64 one."""
+    rng = np.random.default_rng(9)
+    n, N = 6, 8
+    p = np.concatenate([rng.uniform(0, 5, (n, 1)), np.tile(rng.normal(size=N), (n, 1))], axis=1)
+    th0 = rng.uniform(0, 2 * np.pi, (n, N))
+    kw = dict(neq=N, npar=N + 1, nchunks=5)
+    o = Oracle("kuramoto")
+    dp = o.run(5, np.zeros(n), th0, p, dt=0.01, ksteps=20, counters=np.zeros(n), **kw, **TOL)
+    ref = o.run(2, np.zeros(n), th0, p, dt=1e-4, ksteps=2000, **kw)
+    assert rel(dp.records, ref.records, floor=1.0) < 1e-7
+    assert (dp.newton_passes < 5 * 20).all()  # far fewer steps than the fixed-step grid
+    t0, y0, pp = inputs(4, 10)
+    f64 = Oracle("oculomotor").run(5, t0, y0, pp, neq=6, npar=6, dt=1e-3, ksteps=50, nchunks=2,
+                                   counters=np.zeros(4), rtol=1e-5, atol=1e-7)
+    f32 = Oracle("oculomotor", "fp32").run(5, t0, y0, pp, neq=6, npar=6, dt=1e-3, ksteps=50, nchunks=2,
+                                           counters=np.zeros(4), rtol=1e-5, atol=1e-7)
+    assert (f32.flags == 0).all() and rel(f32.records, f64.records, floor=0.1) < 1e-2
+
+
 def test_program_carries_tolerances():
     sim = Integrator(system_path("oculomotor"), "dp45", dt=1e-3, tspan=0.1, ksteps=10, neq=6, npar=6, orbits=4,
                      rtol=2.5e-7, atol=1e-11, max_steps=777)
