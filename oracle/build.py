@@ -101,13 +101,19 @@ def _stamp_ok(target: str, digest: str) -> bool:
     return os.path.exists(target) and os.path.exists(stamp) and open(stamp).read() == digest
 
 
+def build_digest(cmd: list[str], source: str, header_dir: str = HERE) -> str:
+    """What a build stamp records: the command, the unit, and the text of the
+    oracle headers (the unit only names the headers it includes)."""
+    headers = "".join(open(os.path.join(header_dir, h)).read() for h in sorted(os.listdir(header_dir))
+                      if h.endswith(".h"))
+    return hashlib.sha256((" ".join(cmd) + "\0" + source + "\0" + headers).encode()).hexdigest()
+
+
 def _compile(source: str, target: str, extra: list[str]) -> str:
     os.makedirs(os.path.dirname(target), exist_ok=True)
     flags = CFLAGS if "-ffp-contract=fast" not in extra else [f for f in CFLAGS if f != "-ffp-contract=off"]
     cmd = ["gcc"] + flags + ["-I", HERE] + extra + ["-x", "c", "-", "-o", target, "-lm"]
-    # the unit only names the headers it includes: their text goes into the digest too
-    headers = "".join(open(os.path.join(HERE, h)).read() for h in sorted(os.listdir(HERE)) if h.endswith(".h"))
-    digest = hashlib.sha256((" ".join(cmd) + "\0" + source + "\0" + headers).encode()).hexdigest()
+    digest = build_digest(cmd, source)
     if _stamp_ok(target, digest):
         return target
     proc = subprocess.run(cmd, input=source.encode(), capture_output=True)

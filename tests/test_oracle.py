@@ -145,3 +145,21 @@ def test_restatement_equals_reference_build(oculomotor, solver):
     a = oculomotor.run(solver, np.zeros(n), y0, p, counters=cnt, orbit_offset=3, **kw)
     b = ReferenceBuild("oculomotor", solver).run(np.zeros(n), y0, p, counters=cnt, orbit_offset=3, **kw)
     np.testing.assert_array_equal(a.records, b.records)
+
+
+def test_oracle_build_stamp_covers_headers(tmp_path):
+    """A change to an oracle header (oracle_solvers.h, oracle_prelude.h) must
+    rebuild the oracle libraries, although the compiled unit only names them."""
+    import shutil
+
+    from oracle import build
+
+    for h in os.listdir(os.path.dirname(build.__file__)):
+        if h.endswith(".h"):
+            shutil.copy(os.path.join(os.path.dirname(build.__file__), h), tmp_path / h)
+    cmd, unit = ["gcc", "-O2"], '#include "oracle_solvers.h"\n'
+    before = build.build_digest(cmd, unit, str(tmp_path))
+    assert build.build_digest(cmd, unit, str(tmp_path)) == before
+    with open(tmp_path / "oracle_solvers.h", "a") as f:
+        f.write("\n/* edited */\n")
+    assert build.build_digest(cmd, unit, str(tmp_path)) != before
