@@ -4,7 +4,9 @@ Workload (one "step" = one full integration of one batch of orbits):
   oculomotor model (6 states, 6 parameters), RK4, 2^20 orbits per GPU,
   parameters uniform within +-50% of the nominal values (seeded), y0 = the
   reference example's initial state, dt = 1e-3, 10^4 steps, a record every
-  100 steps (101 records, [record][equation][orbit], FP64).
+  100 steps (101 records, [record][equation][orbit], FP64).  The system file
+  is the reference's own examples/oculomotor.cl, as shipped (the staged copy
+  under baseline/_ref); the package's restated file is a companion line.
 
   value     device-resident: inputs already in HBM, one launch per step,
             CUDA-event time of that launch (L2 flushed between steps).
@@ -18,7 +20,9 @@ Workload (one "step" = one full integration of one batch of orbits):
   cpu_baseline  the reference's kernels compiled as C (oracle/_ref), OpenMP over
             all host cores, on an orbit subsample of the same workload.
 
---impl reference runs only that CPU implementation of the path (rank 0).
+--impl reference runs only that CPU implementation of the path (rank 0), on
+the cpu_baseline leg's sample: the first 2^15 orbits with all 10^4 steps per
+step, so that its ms_per_step is the measured time of that sample.
 Under torchrun each rank integrates its own 2^20 orbits (global orbit ids
 offset by rank): weak scaling, no collective on the data path.
 """
@@ -62,17 +66,32 @@ def parse():
     return ap.parse_args()
 
 
+# the reference's own system file, staged verbatim by oracle/build.py
+REFERENCE_SYSTEM = os.path.join(REPO, "baseline", "_ref", "examples", "oculomotor.cl")
+PACKAGE_SYSTEM = os.path.join(REPO, "sodecl_b200", "systems", "oculomotor.cl")
+
+
+def headline_system():
+    """(path, label) of the system file the headline integrates."""
+    if os.path.isfile(REFERENCE_SYSTEM):
+        return REFERENCE_SYSTEM, "reference examples/oculomotor.cl (unmodified)"
+    return PACKAGE_SYSTEM, "sodecl_b200/systems/oculomotor.cl (the reference's file is not staged here)"
+
+
 def workload(n, orbit_offset, seed=2024):
-    """Seeded inputs of orbits [orbit_offset, orbit_offset + n)."""
+    """Seeded inputs of orbits [orbit_offset, orbit_offset + n); pure numpy
+    (sodecl_b200.workloads maps no native library)."""
     from sodecl_b200.workloads import oculomotor
 
     return oculomotor(n, orbit_offset, seed)
 
 
 def config_dict(a, n):
-    return {"workload": "oculomotor-%s-%s" % (a.solver, a.precision), "orbits_per_gpu": n, "nsteps": a.nsteps,
-            "record_every": a.ksteps, "records": a.nsteps // a.ksteps + 1, "dt": a.dt, "neq": 6, "npar": 6,
-            "layout": "[record][equation][orbit]", "l2": "flushed between steps (256 MiB write)"}
+    """The workload; both arms print exactly this."""
+    return {"workload": "oculomotor-%s-%s" % (a.solver, a.precision), "system_file": headline_system()[1],
+            "orbits_per_gpu": n, "nsteps": a.nsteps, "record_every": a.ksteps, "records": a.nsteps // a.ksteps + 1,
+            "dt": a.dt, "neq": 6, "npar": 6, "layout": "[record][equation][orbit]",
+            "l2": "flushed between steps (256 MiB write)"}
 
 
 class ClockSampler:
@@ -145,22 +164,30 @@ def cpu_reference_rate(n, a, cores, kind_pref="reference"):
 
 
 def run_reference_arm(a, rank):
+    """The reference's kernels compiled as C (oracle/_ref), OpenMP over all
+    host cores, on the same sample as the cpu_baseline leg: each step
+    integrates the first a.cpu_orbits orbits through all a.nsteps steps.
+    ms_per_step is that sample's measured time; value is its orbit-steps/s.
+    Imports nothing that maps this library's native code."""
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    n = max(256, a.cpu_orbits // 4)
+    n = min(a.cpu_orbits, a.orbits)
     for _ in range(a.warmup):
         cpu_reference_rate(256, a, cores)
-    vals = []
+    secs = []
+    kind = None
     for _ in range(a.steps):
-        v, secs, kind = cpu_reference_rate(n, a, cores)
-        vals.append(v)
-    value = float(np.mean(vals))
-    sample = "%d of %d orbits x %d steps per step, records every %d" % (n, a.orbits, a.nsteps, a.ksteps)
+        _, sec, kind = cpu_reference_rate(n, a, cores)
+        secs.append(sec)
+    ms = float(np.mean(secs)) * 1e3
+    value = n * a.nsteps / (ms * 1e-3)
+    sample = "the first %d of %d orbits, all %d steps, records every %d, per step (warm-up steps: 256 orbits)" % (
+        n, a.orbits, a.nsteps, a.ksteps)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": a.gpus, "steps": a.steps,
-        "warmup": a.warmup, "ms_per_step": a.orbits * a.nsteps / value * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config_dict(a, a.orbits),
+        "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": config_dict(a, a.orbits),
         "cpu_baseline": {"value": value, "unit": METRIC, "cores": cores, "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
 
@@ -199,7 +226,8 @@ def main():
     offset, n = shard(a.orbits * world, rank, world)
     t0, y0, p = workload(n, offset)
     tspan = a.nsteps * a.dt
-    sim = Integrator(system_path("oculomotor"), a.solver, dt=a.dt, tspan=tspan, ksteps=a.ksteps, neq=6, npar=6,
+    system_file, _ = headline_system()
+    sim = Integrator(system_file, a.solver, dt=a.dt, tspan=tspan, ksteps=a.ksteps, neq=6, npar=6,
                      orbits=n, device=local_rank, precision=a.precision, block=a.block)
     nchunks = sim.num_chunks
     assert nchunks * a.ksteps == a.nsteps, (nchunks, a.ksteps, a.nsteps)
@@ -252,8 +280,8 @@ def main():
     value = world * n * a.nsteps / (ms * 1e-3)
 
     # ---------------- roofline: counted FP64 ops vs measured FMA issue peak
-    fma_rate, _ = sodecl_b200.fma_peak("fp32" if a.precision == "fp32" else "fp64", device=local_rank)
-    peak_tflops = 2.0 * fma_rate / 1e12
+    peaks = {prec: 2.0 * sodecl_b200.fma_peak(prec, device=local_rank)[0] / 1e12 for prec in ("fp64", "fp32")}
+    peak_tflops = peaks[a.precision]
     achieved = RK4_OPS_PER_ORBIT_STEP * n * a.nsteps / (ms * 1e-3) / 1e12 if a.solver == "rk4" else None
     # DRAM bytes per launch: ncu's dram__bytes_read.sum + dram__bytes_write.sum
     # on a 2^18-orbit x 1000-step launch (137.3 MB, 11 records), scaled by
@@ -271,7 +299,8 @@ def main():
                 "unit": "TFLOP/s", "frac": (achieved / peak_tflops) if achieved else None, "traffic": traffic,
                 "algorithmic_bytes": algorithmic_bytes, "hbm_gbs": hbm_gbs,
                 "hbm_frac_of_measured": (hbm_gbs / hbm_peak) if hbm_peak else None,
-                "peak_source": "measured on this GPU: FMA-chain microbenchmark (sodecl_cuda_fma_peak), 2 flops/FMA",
+                "peak_source": "measured on this GPU: FMA-chain microbenchmark (sodecl_cuda_fma_peak, fastest of "
+                               "7 launches), 2 flops/FMA",
                 "ops_per_orbit_step": RK4_OPS_PER_ORBIT_STEP,
                 "fp64_pipe_active": "59.1 % of peak (ncu sm__pipe_fp64_cycles_active, 2^18-orbit x 1000-step "
                                     "launch of this kernel); counted source ops understate the pipe work, exp and "
@@ -314,7 +343,7 @@ def main():
     # companions on single-GPU runs only: under torchrun they would hold every
     # rank's GPU while rank 0 alone works
     if not a.no_extras and world == 1:
-        extras = companions(a, n, dev, stream)
+        extras = companions(a, n, dev, stream, peaks)
         extras["gradient"] = gradient_companion(dev)
         extras["uneven_batch"] = batch_companion(dev)
         extras["stochastic_kuramoto"] = stochastic_kuramoto_companion(dev, stream)
@@ -333,16 +362,16 @@ def main():
                                                                                      a.ksteps, secs)}
     info = sim.kernel_info()
     if rank == 0:
-        cfg = config_dict(a, n)
-        cfg.update({"parallelism": "orbits sharded, %d per GPU" % n, "block": sim.cfg.local_group_size or 128,
-                    "min_blocks_per_sm": sim.cfg.min_blocks_per_sm, "division": sim.division,
-                    "autotuned": tuned is not None, "registers": info["registers"],
-                    "local_bytes": info["local_bytes"], "nan_fraction_final": nan_fraction})
+        launch_info = {"parallelism": "orbits sharded, %d per GPU" % n, "block": sim.cfg.local_group_size or 128,
+                       "min_blocks_per_sm": sim.cfg.min_blocks_per_sm, "division": sim.division,
+                       "autotuned": tuned is not None, "registers": info["registers"],
+                       "local_bytes": info["local_bytes"], "nan_fraction_final": nan_fraction}
         out = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": a.steps,
                "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32", "data": "synthetic",
-               "config": cfg, "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": a.steps,
-               "clocks": clocks.summary(), "wall_s_timed_region": wall, "launch_ms": launch_ms}
+               "config": config_dict(a, n), "launch": launch_info, "roofline": roofline, "cpu_baseline": cpu,
+               "e2e": e2e, "gpu_launches": a.steps, "clocks": clocks.summary(), "wall_s_timed_region": wall,
+               "launch_ms": launch_ms}
         out.update(extras)
         print(json.dumps(out), flush=True)
     sim.close()
@@ -531,29 +560,49 @@ def stochastic_kuramoto_companion(dev, stream, n=1 << 18, N=32, nsteps=2000, kst
     return out
 
 
-def companions(a, n, dev, stream):
+# Counted source-level operations per Newton pass of the implicit midpoint on
+# the reference's oculomotor file (tests/test_opcount.py): the pass that
+# meets the stop test, and a full pass (Jacobian, scaling, banded solve)
+IM_OPS_CONVERGED_PASS, IM_OPS_FULL_PASS = 78, 236
+
+
+def companions(a, n, dev, stream, peaks):
     """Same shape, other settings: the stable step dt=1e-5 (RK4 diverges at
-    1e-3 for most parameter draws), FP32, and implicit midpoint -- with the
+    1e-3 for most parameter draws), FP32, implicit midpoint -- with the
     reference's Newton settings (1e-7, up to 1000 passes) and with the stated
     1e-10 / 10 passes, which the reference's banded solve does not converge
-    within (the orbits that hit the limit are counted)."""
+    within (the orbits that hit the limit are counted) -- all on the
+    headline's system file; and the headline itself on the package's restated
+    system file (sodecl_b200/systems/oculomotor.cl: the same trajectories,
+    with the burst's exp argument selected instead of branched).  Each line
+    carries its counted-operation roofline against the measured FMA peak of
+    its precision."""
     import torch
 
-    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200 import Integrator
 
     out = {}
     t0, y0, p = workload(n, 0)
-    # (name, solver, dt, precision, Newton tolerance, Newton pass limit)
-    cases = [("stable_dt_1e-5", a.solver, 1e-5, a.precision, 1e-7, 1000), ("fp32", a.solver, a.dt, "fp32", 1e-7, 1000),
-             ("fp32_stable_dt_1e-5", a.solver, 1e-5, "fp32", 1e-7, 1000),
-             ("implicit_midpoint", "im", a.dt, "fp64", 1e-7, 1000),
-             ("implicit_midpoint_tol1e-10_max10", "im", a.dt, "fp64", 1e-10, 10),
-             ("implicit_midpoint_fp32_tol1e-10_max10", "im", a.dt, "fp32", 1e-10, 10)]
-    for name, solver, dt, prec, tol, maxit in cases:
-        sim = Integrator(system_path("oculomotor"), solver, dt=dt, tspan=a.nsteps * dt, ksteps=a.ksteps, neq=6,
+    system_file, _ = headline_system()
+    # (name, system file, solver, dt, precision, Newton tolerance, Newton pass limit)
+    cases = [("stable_dt_1e-5", system_file, a.solver, 1e-5, a.precision, 1e-7, 1000),
+             ("fp32", system_file, a.solver, a.dt, "fp32", 1e-7, 1000),
+             ("fp32_stable_dt_1e-5", system_file, a.solver, 1e-5, "fp32", 1e-7, 1000),
+             ("package_system_file", PACKAGE_SYSTEM, a.solver, a.dt, a.precision, 1e-7, 1000),
+             ("package_system_file_stable_dt_1e-5", PACKAGE_SYSTEM, a.solver, 1e-5, a.precision, 1e-7, 1000),
+             ("implicit_midpoint", system_file, "im", a.dt, "fp64", 1e-7, 1000),
+             ("implicit_midpoint_tol1e-10_max10", system_file, "im", a.dt, "fp64", 1e-10, 10),
+             ("implicit_midpoint_fp32_tol1e-10_max10", system_file, "im", a.dt, "fp32", 1e-10, 10)]
+    for name, path, solver, dt, prec, tol, maxit in cases:
+        sim = Integrator(path, solver, dt=dt, tspan=a.nsteps * dt, ksteps=a.ksteps, neq=6,
                          npar=6, orbits=n, precision=prec, newton_tol=tol, newton_max_iter=maxit)
         nrec = sim.num_records
         td, yd, pd = torch.tensor(t0, device=dev), torch.tensor(y0, device=dev), torch.tensor(p, device=dev)
+        tuned = None
+        if solver == a.solver:
+            # tuned like the headline (launch shape and division mode)
+            sim.upload(t0, y0, p)
+            tuned = sim.autotune(sample_orbits=min(n, 1 << 17), sample_steps=200)
         rec = torch.empty((nrec, 6, n), dtype=torch.float64, device=dev)
         passes = torch.zeros(n, dtype=torch.int64, device=dev)
         flags = torch.zeros(n, dtype=torch.int32, device=dev)
@@ -573,13 +622,28 @@ def companions(a, n, dev, stream):
             if it > 0:
                 ms.append(s.elapsed_time(e))
         last = rec[-1].cpu().numpy()
-        entry = {"value": n * a.nsteps / (np.mean(ms) * 1e-3), "unit": METRIC, "dt": dt, "precision": prec,
-                 "solver": solver, "ms": float(np.mean(ms)),
+        t_s = float(np.mean(ms)) * 1e-3
+        entry = {"value": n * a.nsteps / t_s, "unit": METRIC, "dt": dt, "precision": prec, "solver": solver,
+                 "system_file": os.path.relpath(path, REPO), "ms": t_s * 1e3,
                  "nan_fraction_final": float(np.mean(~np.isfinite(last).all(axis=0)))}
+        if tuned:
+            entry["launch"] = tuned
         if solver == "im":
-            entry["newton_passes_per_step"] = float(passes.double().mean().item() / a.nsteps)
+            total_passes = float(passes.double().sum().item())
+            steps = float(n) * a.nsteps
+            entry["newton_passes_per_step"] = total_passes / steps
             entry["newton"] = {"tol": tol, "max_passes": maxit,
                                "orbits_at_pass_limit": float((flags & 1).bool().double().mean().item())}
+            ops = IM_OPS_CONVERGED_PASS * steps + IM_OPS_FULL_PASS * max(0.0, total_passes - steps)
+            basis = ("%d per converged pass + %d per full pass (tests/test_opcount.py), every step's last pass "
+                     "counted as its converged one" % (IM_OPS_CONVERGED_PASS, IM_OPS_FULL_PASS))
+        else:
+            ops = RK4_OPS_PER_ORBIT_STEP * float(n) * a.nsteps
+            basis = "%d per RK4 orbit-step (tests/test_opcount.py)" % RK4_OPS_PER_ORBIT_STEP
+        achieved = ops / t_s / 1e12
+        entry["roofline"] = {"bound": prec, "achieved": achieved, "peak": peaks[prec], "unit": "TFLOP/s",
+                             "frac": achieved / peaks[prec], "ops": basis,
+                             "peak_source": "measured %s FMA issue rate on this GPU, 2 flops/FMA" % prec}
         out[name] = entry
         sim.close()
         del rec

@@ -351,16 +351,30 @@ size_t sodecl_batch_last_error(const sodecl_batch *b, char *buf, size_t n);
  * on a device shares it, each call clears it on `stream` before its launch,
  * and calls that overlap on the GPU race on it.  The first call on a device
  * loads the batch program there and looks up the array's address; make that
- * first call before any stream capture.  Returns after queuing the launch on
- * `stream`; the noise stream of an orbit is keyed by its position. */
+ * first call before any stream capture.  The cached address and the loaded
+ * program belong to the device's context as it was at that first call: after
+ * a cudaDeviceReset in the same process, this entry point must not be used
+ * again.  Returns after queuing the launch on `stream`; the noise stream of
+ * an orbit is keyed by its position.
+ *
+ * Scheduling: within a class, orbits are taken in the caller's order (the
+ * regular entry point sorts each class by decreasing step count so that the
+ * longest orbits start first; this one does not sort, because sorting would
+ * need scratch for the permutation).  Put long orbits first for the same
+ * load balance.
+ *
+ * Inputs are not validated on the host beyond null checks: every pointer but
+ * class_count must be device memory the caller owns, sized for the counts
+ * in class_count; a step count of zero or less takes no step and leaves that
+ * orbit's state unchanged. */
 typedef struct sodecl_batch_io {
-    double *t;                  /* [n] in/out */
-    double *y;                  /* states, in/out */
-    const double *params;       /* parameters */
-    double *counters;           /* [n] in/out, or NULL when no class is stochastic */
-    const int64_t *nsteps;      /* [n] */
-    int64_t *newton_passes;     /* [n] out, or NULL */
-    int32_t *flags;             /* [n] out, or NULL */
+    double *t;                  /* device, [n] in/out */
+    double *y;                  /* device, states, in/out */
+    const double *params;       /* device, parameters */
+    double *counters;           /* device, [n] in/out, or NULL when no class is stochastic */
+    const int64_t *nsteps;      /* device, [n]; <= 0 takes no step */
+    int64_t *newton_passes;     /* device, [n] out, or NULL */
+    int32_t *flags;             /* device, [n] out, or NULL */
     const int64_t *class_count; /* host, one count per class */
 } sodecl_batch_io;
 
@@ -389,8 +403,10 @@ int sodecl_cuda_division_check(int device, int64_t pairs, uint64_t seed, int64_t
                                double *first_b);
 
 /* Issue-rate microbenchmark of the FP64 (precision 0) or FP32 (1) FMA pipe:
- * independent FMA chains on every SM, timed with CUDA events.  Writes the
- * FMA instructions per second summed over all lanes (one FMA = 2 flops). */
+ * independent FMA chains on every SM, timed with CUDA events, the fastest
+ * of seven launches after two warm-up launches.  Writes the FMA
+ * instructions per second summed over all lanes (one FMA = 2 flops) and
+ * that launch's time. */
 int sodecl_cuda_fma_peak(int device, int32_t precision, double *fma_per_s, double *ms);
 
 #ifdef __cplusplus

@@ -13,6 +13,13 @@ Two kinds of shared library come out of this script:
   front and ref_driver.c behind.  Only built where the reference checkout is
   present; the sources are piped to gcc and never copied into this repository.
 
+Where the checkout is present this script also stages verbatim copies of the
+reference's user-facing files (its example system files, its Python layer,
+its known-answer tests and their golden data) under the git-ignored
+``baseline/_ref/``, for the GPU machines, which have no checkout: the tests
+run them unchanged through this library, and bench.py integrates the
+reference's own oculomotor system file.
+
 Both are built with ``-ffp-contract=off`` (x86-64 baseline has no FMA, so this
 only makes the intent explicit) and OpenMP over orbits.
 """
@@ -29,7 +36,19 @@ REPO = os.path.dirname(HERE)
 BUILD_DIR = os.path.join(HERE, "_build")
 REF_DIR = os.path.join(HERE, "_ref")
 SYSTEMS_DIR = os.path.join(REPO, "sodecl_b200", "systems")
+# The reference checkout this recipe reads (read-only); SODECL_REFERENCE_ROOT
+# overrides it.  Nothing else in the repository names this location: tests,
+# smoke() and bench.py read the staged copy under baseline/_ref.
 REFERENCE_ROOT = os.environ.get("SODECL_REFERENCE_ROOT", "/root/reference")
+# Verbatim copies of the reference's user-facing files (system files, Python
+# layer, known-answer tests and their golden data), git-ignored, so that the
+# machines that run the GPU tests and the benchmark -- which have no
+# reference checkout -- can run them unchanged through this library.
+STAGED_ROOT = os.path.join(REPO, "baseline", "_ref")
+STAGED_FILES = ["LICENSE", "examples/oculomotor.cl", "examples/kuramoto.cl", "tests/oculomotor.cl",
+                "tests/kuramoto.cl", "tests/sodecl_python_tests.py", "tests/data/oculomotor_euler.pkl",
+                "tests/data/oculomotor_rk.pkl", "tests/data/oculomotor_ie.pkl", "tests/data/oculomotor_im.pkl",
+                "interfaces/python/sodecl.py"]
 
 CFLAGS = ["-O2", "-std=gnu11", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off",
           "-Wno-unused-variable", "-Wno-unused-but-set-variable"]
@@ -197,6 +216,22 @@ def reference_available() -> bool:
     return os.path.isdir(os.path.join(REFERENCE_ROOT, "src", "kernels"))
 
 
+def stage_reference_inputs() -> list[str]:
+    """Copy STAGED_FILES from the reference checkout to baseline/_ref,
+    byte for byte (rewritten only when they differ)."""
+    out = []
+    for rel in STAGED_FILES:
+        src = os.path.join(REFERENCE_ROOT, rel)
+        dst = os.path.join(STAGED_ROOT, rel)
+        data = open(src, "rb").read()
+        if not os.path.exists(dst) or open(dst, "rb").read() != data:
+            os.makedirs(os.path.dirname(dst), exist_ok=True)
+            with open(dst, "wb") as f:
+                f.write(data)
+        out.append(dst)
+    return out
+
+
 def build_all(verbose: bool = False) -> list[str]:
     built = []
     for fname in sorted(os.listdir(SYSTEMS_DIR)):
@@ -204,14 +239,17 @@ def build_all(verbose: bool = False) -> list[str]:
             for prec in ("fp64", "fp32") + (("fp64fma", "fp32fma") if cpu_has_fma() else ()):
                 built.append(build_restatement(os.path.join(SYSTEMS_DIR, fname), fname[:-3], prec))
     if reference_available():
+        built += stage_reference_inputs()
         for system, solver in REFERENCE_BUILDS:
             built.append(build_reference(system, solver))
         built.append(build_reference_threefry())
         # the reference's own example system files through the restatement,
         # to show the package's system files are faithful restatements
+        # (with FMA contraction too: the noise floor of parity runs on them)
         for system in ("oculomotor", "kuramoto"):
-            built.append(build_restatement(os.path.join(REFERENCE_ROOT, "examples", system + ".cl"),
-                                           "refsys_" + system, "fp64", out_dir=REF_DIR))
+            for prec in ("fp64",) + (("fp64fma",) if cpu_has_fma() else ()):
+                built.append(build_restatement(os.path.join(REFERENCE_ROOT, "examples", system + ".cl"),
+                                               "refsys_" + system, prec, out_dir=REF_DIR))
     if verbose:
         for b in built:
             print("built", os.path.relpath(b, REPO))

@@ -70,6 +70,49 @@ using std::exp; using std::log; using std::sin; using std::cos; using std::sqrt;
 static long long total() { return Counted::add + Counted::mul + Counted::div + Counted::fun; }
 static void reset() { Counted::add = Counted::mul = Counted::div = Counted::fun = 0; }
 
+#ifdef HAS_JACOBIAN
+// One Newton pass of the reference's implicit solvers, written out with the
+// counting type in the order of src/kernels/ie.cl:50-105 (implicit Euler,
+// midpoint = false) and src/kernels/im.cl:43-106 (implicit midpoint).  dt
+// stands for the program's literal _m_dt_ (a plain double); converged = the
+// pass that meets the stop test and returns before the Jacobian.
+static long long newton_pass_ops(bool midpoint, bool converged, Counted *y, Counted *p, double dt)
+{
+    const int n = NUMEQ;
+    Counted guess[NUMEQ], mid[NUMEQ], f[NUMEQ], r[NUMEQ], jac[NUMEQ][NUMEQ], a[NUMEQ], b[NUMEQ], c[NUMEQ], x[NUMEQ];
+    for (int i = 0; i < n; ++i) guess[i] = y[i] + Counted(1e-3 * (i + 1)).v;  // an iterate away from y
+    reset();
+    if (midpoint)
+        for (int i = 0; i < n; ++i) mid[i] = (y[i] + guess[i]) * 0.5;  // im.cl:67-70
+    sode_system(Counted(0.0), midpoint ? mid : guess, f, p);
+    for (int i = 0; i < n; ++i) r[i] = guess[i] - y[i] - f[i] * dt;   // ie.cl:56, im.cl:47
+    Counted err(0.0);
+    for (int i = 0; i < n; ++i) err = midpoint ? err + r[i] * r[i] : err + fabs(r[i]);
+    if (midpoint) err = sqrt(err);                                    // im.cl:76-82, ie.cl:73-78
+    if (converged) return total();
+    calc_jacobian(midpoint ? mid : guess, jac, p);
+    for (int i = 0; i < n; ++i) {                                     // ie.cl:84-92, im.cl:86-93
+        for (int j = 0; j < n; ++j) jac[i][j] = jac[i][j] * (midpoint ? -0.50 : -1.00) * dt;
+        jac[i][i] = jac[i][i] + 1;
+    }
+    // the banded solve, ie.cl:10-48 (band copies are not arithmetic)
+    for (int i = 0; i < n; ++i) {
+        a[i] = (i < n - 2) ? jac[i][i + 1] : Counted(0.0);
+        c[i] = (i < n - 1) ? jac[i + 1][i] : Counted(0.0);
+        b[i] = jac[i][i];
+    }
+    for (int i = 1; i < n; ++i) {
+        Counted m = a[i] / b[i - 1];
+        b[i] = b[i] - m * c[i - 1];
+        r[i] = r[i] - m * r[i - 1];
+    }
+    x[n - 1] = r[n - 1] / b[n - 1];
+    for (int i = n - 2; i >= 0; --i) x[i] = (r[i] - c[i] * x[i + 1]) / b[i];
+    for (int i = 0; i < n; ++i) guess[i] = guess[i] - x[i];          // ie.cl:95-98
+    return total();
+}
+#endif
+
 int main(int argc, char **argv)
 {
     // argv: NUMEQ state values then NUMPAR parameter values
@@ -90,6 +133,10 @@ int main(int argc, char **argv)
     calc_jacobian(y, jac, p);
     std::printf("jacobian %lld add %lld mul %lld div %lld fun %lld\n", total(), Counted::add, Counted::mul,
                 Counted::div, Counted::fun);
+    std::printf("ie_pass_converged %lld\n", newton_pass_ops(false, true, y, p, 1e-3));
+    std::printf("ie_pass_full %lld\n", newton_pass_ops(false, false, y, p, 1e-3));
+    std::printf("im_pass_converged %lld\n", newton_pass_ops(true, true, y, p, 1e-3));
+    std::printf("im_pass_full %lld\n", newton_pass_ops(true, false, y, p, 1e-3));
 #endif
     return 0;
 }

@@ -7,7 +7,17 @@ Native parts (built in-tree by sodecl_b200/build.py):
 
 Python: `Integrator` (numpy API), `sodecl.sodecl(...)` (the reference's
 function), `system_path(name)` for the bundled system files.
+
+The names below load libsodecl_cuda.so on first use, not at import, so that a
+module of this package that needs no GPU (the seeded workload generators in
+`workloads`) can be imported without mapping the library.
 """
-from .api import Integrator, fma_peak, noise_stream, system_path  # noqa: F401
+import importlib
 
 __all__ = ["Integrator", "fma_peak", "noise_stream", "system_path"]
+
+
+def __getattr__(name):
+    if name in __all__:
+        return getattr(importlib.import_module(".api", __name__), name)
+    raise AttributeError("module %r has no attribute %r" % (__name__, name))

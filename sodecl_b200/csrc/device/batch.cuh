@@ -80,8 +80,9 @@ __device__ __forceinline__ void sodecl_class_run(const sodecl_batch_args &a, con
                 sodecl_advance(t, y, p, a.orbit_id ? a.orbit_id[item] : item, counter, passes, capped);
                 --left;
             }
-            if (left == 0) {
-                // store this orbit, take the next one
+            if (left <= 0) {
+                // store this orbit, take the next one (a count below zero
+                // takes no step, like zero)
                 const long long j = item - begin;
                 a.t[item] = (double)t;
                 bool finite = true;

@@ -1,7 +1,7 @@
 // Counter-based Gaussian noise for the Euler-Maruyama solver.
 //
 // Shared, as text, by the NVRTC programs (embedded by the build) and by the
-// statically compiled test kernels in noise_kernels.cu, so both run the same
+// statically compiled test kernels in aux_kernels.cu, so both run the same
 // code.  Self-contained: no includes, usable under NVRTC and nvcc.
 //
 // Generator: Threefry-2x64 with 20 rounds (Salmon, Moraes, Dror, Shaw,

@@ -1,7 +1,7 @@
 """Regenerates the golden fixtures in this directory.
 
-Run in a checkout next to the reference (default /root/reference; override
-with SODECL_REFERENCE_ROOT) after `python oracle/build.py`:
+Run where the reference checkout is present (its location is the one
+oracle/build.py reads, REFERENCE_ROOT there) after `python oracle/build.py`:
 
     python tests/golden/make_golden.py
 
@@ -24,8 +24,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, REPO)
-REFERENCE_ROOT = os.environ.get("SODECL_REFERENCE_ROOT", "/root/reference")
 
+from oracle.build import REFERENCE_ROOT  # noqa: E402
 from oracle.oracle import ReferenceBuild, num_chunks  # noqa: E402
 
 OCULOMOTOR_NOMINAL = [120.0, 1.5, 0.0045, 0.05, 600.0, 9.0]

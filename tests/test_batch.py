@@ -239,3 +239,64 @@ def test_batch_lanes_classes_match_single_system_kernel_bit_for_bit():
         assert t[i] == tt
         if nnoi:
             assert cnt[i] == cc
+
+
+def assert_batch_final_states_match_oracle(classes, cls, nsteps, t0, y0, p, counters, t, y, cnt, per_class, seed):
+    """Samples up to `per_class` orbits (with steps) of every class and checks
+    their final states against the oracle run at each orbit's own step count
+    (noise keyed by the orbit's index, as the batch keys it), within the
+    floor-based tolerance of tests/parity.py."""
+    from oracle.oracle import Oracle
+    from parity import assert_parity
+
+    rng = np.random.default_rng(seed)
+    for k, (system, solver, neq, npar, nnoi, dt) in enumerate(classes):
+        members = np.nonzero((cls == k) & (nsteps > 0))[0]
+        assert members.size > 0, "class %d has no orbit with steps" % k
+        pick = np.sort(rng.choice(members, min(per_class, members.size), replace=False))
+        solver_id = {"se": 0, "euler": 1, "rk4": 2, "ie": 3, "im": 4}[solver]
+        want, alt = np.empty((1, neq, pick.size)), np.empty((1, neq, pick.size))
+        for j, i in enumerate(pick):
+            kw = dict(neq=neq, npar=npar, nnoi=nnoi, dt=dt, ksteps=int(nsteps[i]), nchunks=1, records=False,
+                      counters=[counters[i]] if nnoi else None, orbit_offset=int(i))
+            r = Oracle(system).run(solver_id, [t0[i]], [y0[i]], [p[i]], **kw)
+            a = Oracle(system, "fp64fma").run(solver_id, [t0[i]], [y0[i]], [p[i]], **kw)
+            want[0, :, j], alt[0, :, j] = r.y[0], a.y[0]
+            assert t[i] == r.t[0]
+            if nnoi:
+                assert cnt[i] == r.counters[0]
+        got = np.stack([y[i] for i in pick], axis=1)[None]
+        assert_parity("batch class %d (%s %s N=%d) vs oracle" % (k, system, solver, neq), got, want, alt)
+
+
+@pytest.mark.gpu
+def test_batch_classes_match_oracle():
+    """Every class of a batch (one lane per orbit: Kuramoto Euler / RK4 /
+    implicit Euler / Euler-Maruyama, oculomotor RK4 / implicit Euler /
+    implicit midpoint) against the CPU oracle, not only against the
+    single-system kernel.  Kuramoto implicit Euler uses this library's
+    Kuramoto file, which adds the calc_jacobian the reference's lacks."""
+    n = 3000
+    cls, nsteps, t0, y0, p, counters = make_items(n, 21)
+    b = make_batch()
+    b.set_items(cls, nsteps, t0, y0, p, counters)
+    b.run(graph=True)
+    t, y, cnt, _, _ = b.results()
+    assert_batch_final_states_match_oracle(CLASSES, cls, nsteps, t0, y0, p, counters, t, y, cnt, 12, 22)
+
+
+@pytest.mark.gpu
+def test_batch_lanes_classes_match_oracle():
+    """The wide classes that run several lanes per orbit (N up to 64,
+    implicit Euler and midpoint among them) against the CPU oracle."""
+    classes = [c[:6] for c in LANES_CLASSES]
+    b = Batch()
+    for system, solver, neq, npar, nnoi, dt, lanes in LANES_CLASSES:
+        b.add_class(system_path(system), solver, neq=neq, npar=npar, nnoi=nnoi, dt=dt, lanes=lanes)
+    b.compile()
+    n = 700
+    cls, nsteps, t0, y0, p, counters = make_items(n, 23, classes=classes, steps=(1, 7, 50, 123))
+    b.set_items(cls, nsteps, t0, y0, p, counters)
+    b.run(graph=True)
+    t, y, cnt, _, _ = b.results()
+    assert_batch_final_states_match_oracle(classes, cls, nsteps, t0, y0, p, counters, t, y, cnt, 6, 24)

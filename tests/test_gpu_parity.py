@@ -29,6 +29,7 @@ import sodecl_b200
 from sodecl_b200 import _native as N
 from sodecl_b200 import Integrator, system_path
 from oracle.oracle import Oracle, printed_dt, to_reference_layout
+from parity import RTOL, assert_parity, rel_error  # noqa: F401
 
 pytestmark = pytest.mark.gpu
 
@@ -36,38 +37,12 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 NOMINAL = np.array([120.0, 1.5, 0.0045, 0.05, 600.0, 9.0])
 Y0 = np.array([0.0, 0.0, 0.0, 0.0, 0.0, 2.0])
-RTOL = 1e-12
 
 
 @pytest.fixture(scope="module", autouse=True)
 def _need_gpu():
     if N.device_count() < 1:
         pytest.fail("no CUDA device: the gpu tests need a B200")
-
-
-def rel_error(got, want):
-    """(max error over elements finite in both, count of NaN/Inf mismatches)."""
-    got, want = np.asarray(got, dtype=float), np.asarray(want, dtype=float)
-    fin_w, fin_g = np.isfinite(want), np.isfinite(got)
-    both = fin_w & fin_g
-    axes = tuple(i for i in range(want.ndim) if i != 1)
-    scale = np.max(np.where(fin_w, np.abs(want), 0.0), axis=axes, keepdims=True)
-    den = np.abs(want) + 1e-3 * scale + 1e-300
-    err = np.where(both, np.abs(np.where(both, got, 0) - np.where(both, want, 0)) / den, 0.0)
-    return float(err.max()) if err.size else 0.0, int(np.count_nonzero(fin_w != fin_g))
-
-
-def assert_parity(label, got, want, alt, rtol=RTOL):
-    """got vs want within max(rtol, 10 x floor), floor = distance of `alt`
-    (a second oracle build) from `want`."""
-    floor, floor_nan = rel_error(alt, want)
-    err, nan_mismatch = rel_error(got, want)
-    tol = max(rtol, 10 * floor)
-    print("%s: error %.3g (floor %.3g, tolerance %.3g), NaN mismatches %d (floor %d)"
-          % (label, err, floor, tol, nan_mismatch, floor_nan))
-    assert err <= tol
-    assert nan_mismatch <= 10 * floor_nan
-    return err
 
 
 def run_gpu(system, solver, t0, y0, p, counters=None, **kw):

@@ -99,3 +99,49 @@ def test_noalloc_batch_run_matches_regular_entry_point_twice():
         np.testing.assert_array_equal(c_d.cpu().numpy(), c_ref)
         np.testing.assert_array_equal(passes_d.cpu().numpy(), passes_ref)
         np.testing.assert_array_equal(flags_d.cpu().numpy(), flags_ref)
+
+
+@pytest.mark.gpu
+def test_noalloc_step_count_below_zero_takes_no_step():
+    """The allocation-free launch reads step counts from the caller's device
+    memory, which the host never inspects: a count below zero must take no
+    step, like zero, and the launch must return.  Every orbit with such a
+    count keeps its state; the others equal the regular entry point's run
+    with those counts at zero."""
+    torch = pytest.importorskip("torch")
+    if N.device_count() < 1:
+        pytest.fail("no CUDA device")
+    per_class = [64, 64, 32, 32, 32, 32]
+    cls, steps, t0, y0, p, counters = class_grouped_items(per_class, 5)
+    negative = np.zeros(len(cls), bool)
+    negative[::7] = True
+    steps_zeroed = np.where(negative, 0, steps)
+
+    ref = build_batch()
+    ref.set_items(cls, steps_zeroed, t0, y0, p, counters)
+    ref.run(graph=False)
+    t_ref, y_ref, c_ref, passes_ref, _ = ref.results()
+
+    b = build_batch()
+    dev = torch.device("cuda", 0)
+    t_d = torch.tensor(t0, device=dev)
+    y_d = torch.tensor(np.concatenate(y0), device=dev)
+    p_d = torch.tensor(np.concatenate(p), device=dev)
+    c_d = torch.tensor(counters, device=dev)
+    s_d = torch.tensor(np.where(negative, -1, steps).astype(np.int64), device=dev)
+    passes_d = torch.zeros(len(cls), dtype=torch.int64, device=dev)
+    io = N.BatchIO()
+    io.t, io.y, io.params, io.counters = t_d.data_ptr(), y_d.data_ptr(), p_d.data_ptr(), c_d.data_ptr()
+    io.nsteps, io.newton_passes, io.flags = s_d.data_ptr(), passes_d.data_ptr(), None
+    counts = np.array(per_class, dtype=np.int64)
+    io.class_count = counts.ctypes.data
+    stream = torch.cuda.current_stream(dev)
+    assert N.lib.sodecl_batch_run_noalloc(b._b, C.byref(io), C.c_void_p(stream.cuda_stream)) == N.OK
+    torch.cuda.synchronize()
+    t_got = t_d.cpu().numpy()
+    np.testing.assert_array_equal(t_got, t_ref)
+    np.testing.assert_array_equal(t_got[negative], t0[negative])
+    np.testing.assert_array_equal(y_d.cpu().numpy(), np.concatenate(y_ref))
+    np.testing.assert_array_equal(c_d.cpu().numpy(), c_ref)
+    np.testing.assert_array_equal(passes_d.cpu().numpy(), passes_ref)
+    assert (passes_d.cpu().numpy()[negative] == 0).all()
