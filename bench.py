@@ -338,6 +338,11 @@ def main():
                "pinned host buffers"}
         assert np.array_equal(host_out[-1].numpy(), rec_last, equal_nan=True)
 
+    # ---------------- the drop-in path end to end (single-GPU runs)
+    e2e_dropin = None
+    if not a.no_e2e and world == 1:
+        e2e_dropin = dropin_e2e(a, n, t0, y0, p, rec_last)
+
     # ---------------- companions: stable step, fp32, implicit midpoint
     extras = {}
     # companions on single-GPU runs only: under torchrun they would hold every
@@ -370,13 +375,52 @@ def main():
                "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32", "data": "synthetic",
                "config": config_dict(a, n), "launch": launch_info, "roofline": roofline, "cpu_baseline": cpu,
-               "e2e": e2e, "gpu_launches": a.steps, "clocks": clocks.summary(), "wall_s_timed_region": wall,
+               "e2e": e2e, "e2e_dropin": e2e_dropin, "gpu_launches": a.steps, "clocks": clocks.summary(), "wall_s_timed_region": wall,
                "launch_ms": launch_ms}
         out.update(extras)
         print(json.dumps(out), flush=True)
     sim.close()
     if dist is not None:
         dist.destroy_process_group()
+
+
+def dropin_e2e(a, n, t0, y0, p, rec_last, reps=3):
+    """The headline through the reference's Python entry point on this
+    library, sodecl_b200.sodecl.sodecl(platform, device, system file, initx,
+    params, solver, orbits, nequat, nnoise, dt, tspan, ksteps, local size):
+    per call a new manager (program from the on-disk cache), upload from
+    pageable numpy arrays, the run, and the records in a new pageable numpy
+    array -- as a user of the reference calls it, with its default launch
+    shape (local size 0, no tuning).  Wall clock per call, median of `reps`
+    after one untimed call."""
+    import contextlib
+    import io
+
+    from sodecl_b200.sodecl import sodecl
+
+    system_file, _ = headline_system()
+    solver = {"euler": 1, "rk4": 2, "ie": 3, "im": 4}[a.solver]
+    tspan = a.nsteps * a.dt
+
+    def call():
+        with contextlib.redirect_stdout(io.StringIO()):  # the manager prints its runtime line
+            return sodecl(0, 0, system_file, y0, p, solver, n, 6, 0, a.dt, tspan, a.ksteps, 0,
+                          precision=0 if a.precision == "fp64" else 1)
+
+    _, res = call()
+    secs = []
+    for _ in range(reps):
+        w0 = time.perf_counter()
+        _, res = call()
+        secs.append(time.perf_counter() - w0)
+    # the last record of the drop-in run equals the device-resident run's
+    same = bool(np.array_equal(res[:, -1].reshape(6, n), rec_last, equal_nan=True))
+    s = float(np.median(secs))
+    return {"value": n * a.nsteps / s, "unit": METRIC, "ms_per_step": s * 1e3, "ms_all": [x * 1e3 for x in secs],
+            "h2d_bytes_per_step": int(t0.nbytes + y0.nbytes + p.nbytes), "d2h_bytes_per_step": int(res.nbytes),
+            "records_equal_to_device_run": same,
+            "path": "sodecl_b200.sodecl.sodecl -> sodecl_interface.sodeclcall_array -> sodecl::sodeclmgr -> "
+                    "C ABI; pageable numpy in and out; default launch shape"}
 
 
 def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):

@@ -33,7 +33,11 @@ enum class device_Type : uint64_t { ALL = 0xFFFFFFFFull, CPU = 1ull << 1, GPU = 
 class sodeclmgr {
   public:
     std::vector<double> m_output;  // records, [record][equation][orbit]
-    int m_output_size = 0;
+    // Number of doubles in m_output after a run.  The reference declares this
+    // member as int (and never sets it); 64 bits here, because the records
+    // of large runs pass 2^31 doubles (2^20 orbits x 6 equations x 400
+    // records).
+    int64_t m_output_size = 0;
 
     // kernel_path_str is accepted and ignored (the solvers are built in);
     // sode_system_str is the path of the system file, read at setup.
@@ -71,6 +75,13 @@ class sodeclmgr {
     void set_tolerances(double rtol, double atol, int max_steps);  // solver_Type::DormandPrince
     void set_precision(int precision);  // SODECL_FP64 or SODECL_FP32
     void set_fmad(bool on);
+    // Doubles one run writes (records x equations x orbits); valid after
+    // setup_sode_solver.
+    int64_t output_length() const;
+    // run_sode_solver with the records written to `out` (host or device
+    // memory of at least output_length() doubles) instead of m_output; the
+    // output type is not consulted.  1 = success, 0 = failure.
+    int run_sode_solver_into(double *out, int64_t out_len);
     sodecl_ctx *context() const { return m_ctx; }
     const std::string &last_error() const { return m_error; }
 

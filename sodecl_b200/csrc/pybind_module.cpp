@@ -77,33 +77,59 @@ std::vector<double> sodeclcall(std::vector<double> &a_t0, std::vector<double> &a
     return out;
 }
 
-py::array_t<double> sodeclcall_array(std::vector<double> a_t0, std::vector<double> a_y0, std::vector<double> a_params,
-                                     int a_platform, int a_device, std::string a_system, int a_solver_type, int a_orbits,
-                                     int a_equats, int a_nparams, int a_nnoi, double a_dt, double a_tspan, int a_ksteps,
+using InArray = py::array_t<double, py::array::c_style | py::array::forcecast>;
+
+// sodeclcall with numpy arrays in and out: the inputs are read in place (no
+// per-element conversion to lists) and the records are written by the
+// library straight into a new, uninitialised numpy array -- the device's
+// record stream staged through pinned memory by the library's copy threads
+// while the launches still run.  Returns an empty array on failure.
+py::array_t<double> sodeclcall_array(InArray a_t0, InArray a_y0, InArray a_params, int a_platform, int a_device,
+                                     std::string a_system, int a_solver_type, int a_orbits, int a_equats,
+                                     int a_nparams, int a_nnoi, double a_dt, double a_tspan, int a_ksteps,
                                      int a_local_group_size, int precision, int fmad, double newton_tol,
                                      int newton_max_iter, py::object counters)
 {
-    CallOptions opt;
-    opt.precision = precision;
-    opt.fmad = fmad;
-    opt.newton_tol = newton_tol;
-    opt.newton_max_iter = newton_max_iter;
-    std::vector<double> cnt;
-    if (!counters.is_none()) {
-        cnt = counters.cast<std::vector<double>>();
-        opt.counters = &cnt;
+    if (a_solver_type < 0 || a_solver_type > 4) {
+        std::cout << "Unknown SODE solver selection." << std::endl;
+        return py::array_t<double>(0);
     }
-    auto *out = new std::vector<double>();
+    const py::ssize_t n = a_orbits > 0 ? a_orbits : 0;
+    const bool have_counters = !counters.is_none();
+    InArray cnt;
+    if (have_counters) cnt = InArray::ensure(counters);
+    if (a_t0.size() < n || a_y0.size() < n * std::max(0, a_equats) || a_params.size() < n * std::max(0, a_nparams) ||
+        (have_counters && (!cnt || cnt.size() < n))) {
+        std::cout << "Input arrays are shorter than orbits x sizes." << std::endl;
+        return py::array_t<double>(0);
+    }
+    std::string path = a_system;
+    sodecl::sodeclmgr mgr("kernels", &path[0], static_cast<sodecl::solver_Type>(a_solver_type), a_dt, a_tspan,
+                          a_ksteps, a_equats, a_nparams, a_nnoi, a_orbits, sodecl::output_Type::Array);
+    if (mgr.choose_device(a_platform, sodecl::device_Type::ALL, a_device) == 0)
+        std::cerr << "Error selecting CUDA device!" << std::endl;
+    mgr.set_t0(const_cast<double *>(a_t0.data()));
+    mgr.set_y0(const_cast<double *>(a_y0.data()));
+    mgr.set_params(const_cast<double *>(a_params.data()));
+    mgr.set_local_group_size(a_local_group_size);
+    mgr.set_precision(precision);
+    mgr.set_fmad(fmad != 0);
+    mgr.set_newton(newton_tol, newton_max_iter);
+    if (have_counters) mgr.set_noise_counters(cnt.data());
     bool ok;
     {
         py::gil_scoped_release release;
-        ok = run_call(a_t0, a_y0, a_params, a_platform, a_device, a_system, a_solver_type, a_orbits, a_equats, a_nparams,
-                      a_nnoi, a_dt, a_tspan, a_ksteps, a_local_group_size, opt, *out);
+        ok = mgr.setup_sode_solver() != 0;
     }
-    if (!ok) out->clear();
-    py::capsule owner(out, [](void *p) { delete static_cast<std::vector<double> *>(p); });
-    return py::array_t<double>({static_cast<py::ssize_t>(out->size())}, {static_cast<py::ssize_t>(sizeof(double))},
-                               out->data(), owner);
+    if (!ok) return py::array_t<double>(0);
+    py::array_t<double> out(static_cast<py::ssize_t>(mgr.output_length()));
+    double *dst = out.mutable_data();
+    const int64_t len = out.size();
+    {
+        py::gil_scoped_release release;
+        ok = mgr.run_sode_solver_into(dst, len) != 0;
+    }
+    return ok ? out : py::array_t<double>(0);
 }
 
 }  // namespace

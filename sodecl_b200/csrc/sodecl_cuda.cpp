@@ -13,13 +13,16 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <random>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "program.hpp"
@@ -68,6 +71,32 @@ struct AdjointArgs {
 
 constexpr int kDefaultBlock = 128;
 constexpr int kMaxCopyGroups = 8;
+// Host output in pageable memory: launch groups of about this many record
+// intervals each (at least kMinPageableGroups groups), so that copying out
+// starts early and keeps pace with the launches.
+constexpr int kMinPageableGroups = 16;
+
+// Pinned staging for copies into pageable host memory.  A copy from the
+// device into pageable memory goes through the driver's own small staging
+// buffer on the calling thread.  Instead, kStageWorkers host threads each
+// bring pieces of the records into two pinned slots of their own (one in
+// flight while the other is copied into the destination), so the copies run
+// on several streams and the page faults of a fresh destination are taken
+// by several threads.  The slots are pinned once per process and shared by
+// every context; one run at a time copies through them.
+constexpr int kStageWorkers = 8;
+constexpr size_t kStageSlotBytes = size_t(8) << 20;
+
+struct StagingPool {
+    std::mutex in_use;
+    std::vector<void *> slots;  // 2 per worker, kStageSlotBytes each
+};
+
+StagingPool &staging_pool()
+{
+    static StagingPool pool;
+    return pool;
+}
 
 }  // namespace
 
@@ -209,6 +238,88 @@ int ensure_gpu(sodecl_ctx *ctx)
 }
 
 int lanes_of(const sodecl_cfg &c) { return c.lanes_per_orbit > 1 ? c.lanes_per_orbit : 1; }
+
+// A piece of the record buffer: `count` doubles at element offset `off`,
+// ready once launch group `group` has finished.
+struct Piece {
+    int64_t off;
+    int64_t count;
+    int group;
+};
+
+// Copies the pieces of d_rec into the pageable `out` through the pinned
+// staging pool (kStageWorkers threads, two slots each).  Worker w takes
+// pieces w, w + W, w + 2W, ... (so each worker meets them in the order the
+// launches finish them); for each it queues the copy of its next piece into
+// its other slot before copying the current one out of its slot.  `pool`
+// is locked by the caller.  Returns cudaSuccess or the first error.
+cudaError_t staged_copy(int device, double *out, const double *d_rec, const std::vector<Piece> &pieces,
+                        const std::vector<cudaEvent_t> &done, StagingPool &pool)
+{
+    const int nworkers = static_cast<int>(pool.slots.size() / 2);
+    std::atomic<int> first_error{static_cast<int>(cudaSuccess)};
+    auto note = [&](cudaError_t e) {
+        if (e != cudaSuccess) {
+            int expected = static_cast<int>(cudaSuccess);
+            first_error.compare_exchange_strong(expected, static_cast<int>(e));
+        }
+        return e == cudaSuccess;
+    };
+    auto work = [&](int w) {
+        if (!note(cudaSetDevice(device))) return;
+        cudaStream_t st = nullptr;
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        if (!note(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking))) return;
+        bool ok = note(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming)) &&
+                  note(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+        auto issue = [&](size_t j, int slot) {
+            const Piece &pc = pieces[j];
+            return note(cudaStreamWaitEvent(st, done[pc.group], 0)) &&
+                   note(cudaMemcpyAsync(pool.slots[2 * w + slot], d_rec + pc.off,
+                                        static_cast<size_t>(pc.count) * sizeof(double), cudaMemcpyDeviceToHost, st)) &&
+                   note(cudaEventRecord(ev[slot], st));
+        };
+        size_t j = static_cast<size_t>(w);
+        if (ok && j < pieces.size()) ok = issue(j, 0);
+        for (int k = 0; ok && j < pieces.size(); ++k, j += nworkers) {
+            const size_t next = j + nworkers;
+            if (next < pieces.size() && !issue(next, (k + 1) & 1)) break;
+            if (!note(cudaEventSynchronize(ev[k & 1]))) break;
+            if (first_error.load() != static_cast<int>(cudaSuccess)) break;
+            std::memcpy(out + pieces[j].off, pool.slots[2 * w + (k & 1)],
+                        static_cast<size_t>(pieces[j].count) * sizeof(double));
+        }
+        cudaStreamSynchronize(st);
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+        cudaStreamDestroy(st);
+    };
+    std::vector<std::thread> threads;
+    threads.reserve(nworkers);
+    for (int w = 0; w < nworkers; ++w) threads.emplace_back(work, w);
+    for (auto &t : threads) t.join();
+    return static_cast<cudaError_t>(first_error.load());
+}
+
+// Pins the staging pool's slots on first use; false if pinned memory is not
+// available (the caller then copies without staging).
+bool staging_ready(StagingPool &pool)
+{
+    if (!pool.slots.empty()) return true;
+    const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+    const int workers = std::max(1, std::min<int>(kStageWorkers, static_cast<int>(hw / 2)));
+    for (int k = 0; k < 2 * workers; ++k) {
+        void *p = nullptr;
+        if (cudaHostAlloc(&p, kStageSlotBytes, cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            for (void *q : pool.slots) cudaFreeHost(q);
+            pool.slots.clear();
+            return false;
+        }
+        pool.slots.push_back(p);
+    }
+    return true;
+}
 
 // Whether the system file has the per-row functions lanes per orbit need
 // with this solver.
@@ -535,14 +646,17 @@ int sodecl_cuda_run(sodecl_ctx *ctx, double *out, int64_t out_len)
     a.flags = ctx->d_flags;
 
     cudaPointerAttributes attr{};
-    bool device_out = false;
+    bool device_out = false, pageable_out = false;
     if (out) {
         if (cudaPointerGetAttributes(&attr, out) != cudaSuccess) {
             cudaGetLastError();
             attr.type = cudaMemoryTypeUnregistered;
         }
         device_out = attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+        pageable_out = attr.type == cudaMemoryTypeUnregistered;
     }
+    const auto wall0 = std::chrono::steady_clock::now();
+    bool staged = false;
 
     cudaEvent_t t_begin, t_kernels, t_end;
     SODECL_CUDA_TRY(ctx, cudaEventCreate(&t_begin));
@@ -577,15 +691,30 @@ int sodecl_cuda_run(sodecl_ctx *ctx, double *out, int64_t out_len)
             SODECL_CUDA_TRY(ctx, cudaMalloc(&ctx->d_records, need));
             ctx->d_records_bytes = need;
         }
-        // Launch groups of halving size (half the record intervals, a quarter,
-        // ...; the last takes the rest): each group's records are copied out on
-        // the second stream while later groups compute, and only the last, small
-        // group's copy is left exposed at the end.
+        // Pinned output: launch groups of halving size (half the record
+        // intervals, a quarter, ...; the last takes the rest): each group's
+        // records are copied out on the second stream while later groups
+        // compute, and only the last, small group's copy is left exposed at
+        // the end.  Pageable output: equal groups of at most 1/16 of the
+        // intervals, staged through pinned memory by host threads, which start
+        // on the first group's records and keep pace with the launches.
+        std::unique_lock<std::mutex> pool_lock;
+        StagingPool &pool = staging_pool();
+        if (pageable_out) {
+            pool_lock = std::unique_lock<std::mutex>(pool.in_use);
+            staged = staging_ready(pool);
+            if (!staged) pool_lock.unlock();
+        }
         std::vector<int64_t> first{0};
-        while (first.back() < ctx->nchunks) {
-            const int64_t rest = ctx->nchunks - first.back();
-            const bool last = static_cast<int64_t>(first.size()) == kMaxCopyGroups;
-            first.push_back(first.back() + (last ? rest : std::max<int64_t>(1, (rest + 1) / 2)));
+        if (staged) {
+            const int64_t per = std::max<int64_t>(1, (ctx->nchunks + kMinPageableGroups - 1) / kMinPageableGroups);
+            while (first.back() < ctx->nchunks) first.push_back(std::min<int64_t>(ctx->nchunks, first.back() + per));
+        } else {
+            while (first.back() < ctx->nchunks) {
+                const int64_t rest = ctx->nchunks - first.back();
+                const bool last = static_cast<int64_t>(first.size()) == kMaxCopyGroups;
+                first.push_back(first.back() + (last ? rest : std::max<int64_t>(1, (rest + 1) / 2)));
+            }
         }
         if (first.size() == 1) first.push_back(0);  // no interval: one launch stores the final record
         const int64_t groups = static_cast<int64_t>(first.size()) - 1;
@@ -602,15 +731,34 @@ int sodecl_cuda_run(sodecl_ctx *ctx, double *out, int64_t out_len)
             SODECL_CUDA_TRY(ctx, cudaEventRecord(done[g], ctx->stream));
         }
         SODECL_CUDA_TRY(ctx, cudaEventRecord(t_kernels, ctx->stream));
-        for (int64_t g = 0; g < groups; ++g) {
-            const int64_t r0 = first[g];
-            const int64_t r1 = (g == groups - 1) ? nrec : first[g + 1];
-            SODECL_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy_stream, done[g], 0));
-            SODECL_CUDA_TRY(ctx, cudaMemcpyAsync(out + r0 * rec_elems, d_rec + r0 * rec_elems,
-                                                 static_cast<size_t>((r1 - r0) * rec_elems) * sizeof(double),
-                                                 cudaMemcpyDeviceToHost, ctx->copy_stream));
+        if (staged) {
+            // pieces of at most one slot, in the order the groups finish
+            const int64_t slot_elems = static_cast<int64_t>(kStageSlotBytes / sizeof(double));
+            std::vector<Piece> pieces;
+            for (int64_t g = 0; g < groups; ++g) {
+                const int64_t e0 = first[g] * rec_elems;
+                const int64_t e1 = ((g == groups - 1) ? nrec : first[g + 1]) * rec_elems;
+                for (int64_t e = e0; e < e1; e += slot_elems)
+                    pieces.push_back(Piece{e, std::min(slot_elems, e1 - e), static_cast<int>(g)});
+            }
+            const cudaError_t e = staged_copy(ctx->cfg.device, out, d_rec, pieces, done, pool);
+            if (e != cudaSuccess) {
+                cudaStreamSynchronize(ctx->stream);
+                return cuda_fail(ctx, e, "staged record copy");
+            }
+            pool_lock.unlock();
+            SODECL_CUDA_TRY(ctx, cudaEventRecord(t_end, ctx->stream));
+        } else {
+            for (int64_t g = 0; g < groups; ++g) {
+                const int64_t r0 = first[g];
+                const int64_t r1 = (g == groups - 1) ? nrec : first[g + 1];
+                SODECL_CUDA_TRY(ctx, cudaStreamWaitEvent(ctx->copy_stream, done[g], 0));
+                SODECL_CUDA_TRY(ctx, cudaMemcpyAsync(out + r0 * rec_elems, d_rec + r0 * rec_elems,
+                                                     static_cast<size_t>((r1 - r0) * rec_elems) * sizeof(double),
+                                                     cudaMemcpyDeviceToHost, ctx->copy_stream));
+            }
+            SODECL_CUDA_TRY(ctx, cudaEventRecord(t_end, ctx->copy_stream));
         }
-        SODECL_CUDA_TRY(ctx, cudaEventRecord(t_end, ctx->copy_stream));
     }
     SODECL_CUDA_TRY(ctx, cudaEventSynchronize(t_end));
     SODECL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -618,7 +766,9 @@ int sodecl_cuda_run(sodecl_ctx *ctx, double *out, int64_t out_len)
     SODECL_CUDA_TRY(ctx, cudaEventElapsedTime(&kms, t_begin, t_kernels));
     SODECL_CUDA_TRY(ctx, cudaEventElapsedTime(&tms, t_begin, t_end));
     ctx->last_kernel_ms = kms;
-    ctx->last_total_ms = tms;
+    // the staged copy ends on the host: its total is the wall time
+    ctx->last_total_ms =
+        staged ? std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - wall0).count() : tms;
     return SODECL_OK;
 }
 

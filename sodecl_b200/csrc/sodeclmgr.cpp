@@ -157,7 +157,26 @@ int sodeclmgr::run_sode_solver()
         std::cout << "Error: failed to run the solver: " << m_error << std::endl;
         return 0;
     }
-    m_output_size = static_cast<int>(m_output.size());
+    m_output_size = static_cast<int64_t>(m_output.size());
+    const double walltime = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
+    std::cout << "Compute results runtime: " << walltime << " sec.\n";
+    return 1;
+}
+
+int64_t sodeclmgr::output_length() const
+{
+    return m_ctx ? sodecl_cuda_num_records(m_ctx) * m_cfg.num_equat * m_cfg.list_size : 0;
+}
+
+int sodeclmgr::run_sode_solver_into(double *out, int64_t out_len)
+{
+    if (!m_ctx) return 0;
+    const auto start = std::chrono::steady_clock::now();
+    if (sodecl_cuda_run(m_ctx, out, out_len) != SODECL_OK) {
+        m_error = ctx_error(m_ctx);
+        std::cout << "Error: failed to run the solver: " << m_error << std::endl;
+        return 0;
+    }
     const double walltime = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
     std::cout << "Compute results runtime: " << walltime << " sec.\n";
     return 1;

@@ -159,6 +159,9 @@ def _parse():
     ap.add_argument("--min-blocks", type=int, default=0)
     ap.add_argument("--launches", type=int, default=2)
     ap.add_argument("--max-steps", type=int, default=10000, help="uneven-batch: longest step count")
+    ap.add_argument("--system-file", default=None,
+                    help="oculomotor-*, kuramoto-*, stochastic-kuramoto: integrate this system file instead of "
+                         "the package's (e.g. the reference's own examples/oculomotor.cl)")
     return ap.parse_args()
 
 
@@ -188,7 +191,7 @@ def main():
         system, neq, nnoi = "kuramoto", a.N, 0
     else:
         raise SystemExit("unknown case " + a.case)
-    sim = Integrator(system_path(system), solver, dt=dt, tspan=a.nsteps * dt, ksteps=a.ksteps, neq=neq,
+    sim = Integrator(a.system_file or system_path(system), solver, dt=dt, tspan=a.nsteps * dt, ksteps=a.ksteps, neq=neq,
                      npar=p.shape[1], nnoi=nnoi, orbits=n, precision=a.precision, lanes=a.lanes, block=a.block,
                      division=a.division, min_blocks=a.min_blocks)
     dev = torch.device("cuda", 0)

@@ -269,3 +269,37 @@ def test_gradient_fit_reduces_the_loss():
     print("fit: loss %.3e -> %.3e" % (losses[0], losses[-1]))
     assert np.isfinite(losses).all()
     assert losses[-1] < 0.5 * losses[0]  # measured: 87.1 -> 18.6
+
+
+@pytest.mark.gpu
+def test_adjoint_at_the_fitting_shape_against_dual_numbers():
+    """The fitting configuration itself -- 2^16 orbits, 5000 RK4 steps of
+    dt 1e-5, a record every 100, targets from seeded true parameters plus
+    N(0, 1e-2) noise, gradient at parameters within +-5 % -- and 64 of its
+    orbits (spread over the index range) against the FP64 dual-number
+    reference gradient: per orbit, max |adjoint - reference| over the 12
+    derivatives, relative to the largest |reference|, within 1e-6."""
+    torch = pytest.importorskip("torch")
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.fit import Adjoint
+    from sodecl_b200.workloads import fitting_targets
+
+    n, nsteps, ksteps, dt = 1 << 16, 5000, 100, 1e-5
+    dev = torch.device("cuda")
+    t0, y0, guess, targets = fitting_targets(n, nsteps, ksteps, dt, device=dev)
+    sim = Integrator(system_path("oculomotor"), "rk4", dt=dt, tspan=(nsteps - 0.5) * dt, ksteps=ksteps, neq=6,
+                     npar=6, orbits=n)
+    T = lambda a: torch.tensor(a, device=dev)  # noqa: E731
+    loss, gp, gy, flags = Adjoint(sim)(T(t0), T(y0), T(guess), targets)
+    assert not flags.any()
+    pick = np.linspace(0, n - 1, 64).astype(int)
+    tg = targets.cpu().numpy()[:, :, pick]
+    loss_r, gp_r, gy_r = reference_gradient(system_path("oculomotor"), 2, 6, 6, dt, ksteps, nsteps // ksteps,
+                                            t0[pick], y0[pick], guess[pick], tg)
+    gp, gy = gp.cpu().numpy()[pick], gy.cpu().numpy()[pick]
+    np.testing.assert_allclose(loss.cpu().numpy()[pick], loss_r, rtol=1e-9)
+    err = np.maximum(np.abs(gp - gp_r).max(axis=1) / np.abs(gp_r).max(axis=1),
+                     np.abs(gy - gy_r).max(axis=1) / np.abs(gy_r).max(axis=1))
+    print("adjoint vs dual numbers at 2^16 x 5000, 64 orbits: max %.2e, p99 %.2e, median %.2e"
+          % (err.max(), np.quantile(err, 0.99), np.median(err)))
+    assert err.max() <= 1e-6
