@@ -351,6 +351,7 @@ def main():
         extras = companions(a, n, dev, stream, peaks)
         extras["gradient"] = gradient_companion(dev)
         extras["uneven_batch"] = batch_companion(dev)
+        extras["uneven_batch_full"] = batch_full_companion()
         extras["stochastic_kuramoto"] = stochastic_kuramoto_companion(dev, stream)
         extras["small_kuramoto"] = small_kuramoto_companion(dev, stream)
         try:
@@ -553,6 +554,38 @@ def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
             "tuned_launch": {"block": block, "blocks_per_sm": bps}, "padded_per_class_ms": padded_ms,
             "speedup_vs_padded": padded_ms / batch_ms, "registers": b.kernel_info()["registers"],
             "lanes_per_class": b.lanes}
+
+
+def batch_full_companion(n=1 << 18, max_steps=100000, seed=4):
+    """The uneven sweep at its configured size: 2^18 orbits, step counts
+    log-uniform in [10^2, 10^5] (3.8e9 orbit-steps), the same 12 classes, in
+    one persistent launch (CUDA graph), after the tuner has chosen lanes per
+    class and the launch shape on an eighth of the orbits with their step
+    counts capped at 200.  One timed launch (it takes about a minute; the
+    padded comparison runs on the smaller sample above)."""
+    from sodecl_b200 import system_path
+    from sodecl_b200.batch import Batch
+    from sodecl_b200.workloads import uneven_batch
+
+    classes, cls, steps, y0, p, rng = uneven_batch(n, max_steps, seed)
+    b = Batch()
+    for system, solver, neq, npar, dt in classes:
+        b.add_class(system_path(system), solver, neq=neq, npar=npar, dt=dt)
+    b.compile()
+    sample = rng.choice(n, n // 8, replace=False)
+    b.set_items(cls[sample], np.minimum(steps[sample], 200), np.zeros(sample.size), [y0[i] for i in sample],
+                [p[i] for i in sample])
+    block, bps, _ = b.tune()
+    b.set_items(cls, steps, np.zeros(n), y0, p)
+    b.set_launch(block, bps)
+    ms = b.run(graph=True)
+    _, _, _, _, flags = b.results()
+    useful = int(steps.sum())
+    return {"orbits": n, "classes": len(classes), "steps": "log-uniform [100, %d]" % max_steps,
+            "orbit_steps": useful, "batch_ms": ms, "value": useful / (ms * 1e-3), "unit": METRIC,
+            "tuned_launch": {"block": block, "blocks_per_sm": bps}, "lanes_per_class": b.lanes,
+            "registers": b.kernel_info()["registers"], "orbits_flagged": int((flags != 0).sum()),
+            "launches_timed": 1}
 
 
 def stochastic_kuramoto_companion(dev, stream, n=1 << 18, N=32, nsteps=2000, ksteps=200, seed=3):

@@ -96,18 +96,20 @@ bool lanes_fit(const sodecl_b200::ProgramSpec &s)
     return (32 / s.lanes) * sodecl_b200::lanes_slot_words(s) * sizeof(double) * 2 <= sodecl_b200_batch::kSharedCap;
 }
 
-// Rebuilds the program with these lanes per orbit per class (no-op when they
-// are the current ones) and loads it in place of the current one.
-int load_lanes(sodecl_batch *b, const std::vector<int> &lanes)
+// Rebuilds the program with these lanes per orbit per class and this
+// register cap (no-op when they are the current ones) and loads it in place
+// of the current one.
+int load_program(sodecl_batch *b, const std::vector<int> &lanes, int reg_blocks)
 {
-    bool same = true;
+    bool same = reg_blocks == b->reg_blocks;
     for (size_t k = 0; k < b->classes.size(); ++k) same = same && b->classes[k].def.spec.lanes == lanes[k];
     if (same && b->prog) return SODECL_OK;
     for (size_t k = 0; k < b->classes.size(); ++k) b->classes[k].def.spec.lanes = lanes[k];
+    b->reg_blocks = reg_blocks;
     std::vector<sodecl_b200::BatchClass> defs;
     for (const auto &c : b->classes) defs.push_back(c.def);
     try {
-        b->prog = sodecl_b200::build_batch(defs, b->fmad != 0, b->division == SODECL_DIV_RECIPROCAL, 256);
+        b->prog = sodecl_b200::build_batch(defs, b->fmad != 0, b->division == SODECL_DIV_RECIPROCAL, 256, reg_blocks);
     } catch (const std::exception &ex) {
         return b->fail(SODECL_ERR_COMPILE, ex.what());
     }
@@ -237,7 +239,8 @@ int sodecl_batch_compile(sodecl_batch *b)
     std::vector<sodecl_b200::BatchClass> defs;
     for (const auto &c : b->classes) defs.push_back(c.def);
     try {
-        b->prog = sodecl_b200::build_batch(defs, b->fmad != 0, b->division == SODECL_DIV_RECIPROCAL, 256);
+        b->prog = sodecl_b200::build_batch(defs, b->fmad != 0, b->division == SODECL_DIV_RECIPROCAL, 256,
+                                           b->reg_blocks);
     } catch (const std::exception &ex) {
         return b->fail(SODECL_ERR_COMPILE, ex.what());
     }
@@ -473,7 +476,7 @@ int sodecl_batch_tune(sodecl_batch *b, int32_t *block, int32_t *blocks_per_sm, d
             }
             if (!fits || std::find(tried.begin(), tried.end(), lanes) != tried.end()) continue;
             tried.push_back(lanes);
-            int rc = load_lanes(b, lanes);
+            int rc = load_program(b, lanes, b->reg_blocks);
             if (rc != SODECL_OK) return rc;
             rc = sodecl_batch_set_launch(b, std::min(b->block, 128), 0);
             if (rc != SODECL_OK) return rc;
@@ -484,24 +487,38 @@ int sodecl_batch_tune(sodecl_batch *b, int32_t *block, int32_t *blocks_per_sm, d
                 best_lanes = lanes;
             }
         }
-        const int rc = load_lanes(b, best_lanes);
+        const int rc = load_program(b, best_lanes, b->reg_blocks);
         if (rc != SODECL_OK) return rc;
     }
+    // Then the register cap of the program (none, 128 or 85 registers per
+    // thread: one program holds every class, so without a cap the most
+    // demanding class sets the count, and with it the resident warps, for
+    // all) and, for each, the launch shape.
+    std::vector<int> lanes_now;
+    for (const auto &c : b->classes) lanes_now.push_back(c.def.spec.lanes);
+    static const int caps[] = {0, 2, 3};
     static const int shapes[][2] = {{64, 0}, {128, 0}, {256, 0}, {128, 2}, {256, 1}, {64, 4}};
     double best = 1e300;
-    int best_block = b->block, best_bps = b->blocks_per_sm;
-    for (const auto &sh : shapes) {
-        if (sodecl_b200_batch::shared_bytes(b, sh[0]) > sodecl_b200_batch::kSharedCap) continue;
-        int rc = sodecl_batch_set_launch(b, sh[0], sh[1]);
+    int best_block = b->block, best_bps = b->blocks_per_sm, best_cap = b->reg_blocks;
+    for (int cap : caps) {
+        int rc = load_program(b, lanes_now, cap);
         if (rc != SODECL_OK) return rc;
-        rc = sodecl_batch_run(b, 0);
-        if (rc != SODECL_OK) return rc;
-        if (b->last_ms < best) {
-            best = b->last_ms;
-            best_block = sh[0];
-            best_bps = sh[1];
+        for (const auto &sh : shapes) {
+            if (sodecl_b200_batch::shared_bytes(b, sh[0]) > sodecl_b200_batch::kSharedCap) continue;
+            rc = sodecl_batch_set_launch(b, sh[0], sh[1]);
+            if (rc != SODECL_OK) return rc;
+            rc = sodecl_batch_run(b, 0);
+            if (rc != SODECL_OK) return rc;
+            if (b->last_ms < best) {
+                best = b->last_ms;
+                best_block = sh[0];
+                best_bps = sh[1];
+                best_cap = cap;
+            }
         }
     }
+    const int rc = load_program(b, lanes_now, best_cap);
+    if (rc != SODECL_OK) return rc;
     sodecl_batch_set_launch(b, best_block, best_bps);
     if (block) *block = best_block;
     if (blocks_per_sm) *blocks_per_sm = best_bps;

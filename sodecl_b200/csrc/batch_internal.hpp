@@ -74,6 +74,9 @@ struct sodecl_batch {
     int division = SODECL_DIV_RECIPROCAL;
     int block = 128;
     int blocks_per_sm = 0;  // 0 = occupancy limit
+    // register cap of the program: resident blocks of 256 threads the
+    // compiler must allow for (0: none, up to 255 registers per thread)
+    int reg_blocks = 0;
     std::vector<sodecl_b200_batch::Class> classes;
     std::shared_ptr<const sodecl_b200::Program> prog;
     cudaLibrary_t lib = nullptr;

@@ -46,7 +46,102 @@ struct sodecl_batch_args {
 #endif
 
 #ifdef SODECL_BATCH_CLASS_BODY
-#if SODECL_LANES == 1
+// Stores orbit `item` (position j in its class) with its status.
+__device__ __forceinline__ void sodecl_batch_store(const sodecl_batch_args &a, long long item, long long j,
+                                                   long long ybase, real_t t, const real_t *y, double counter,
+                                                   long long passes, int capped)
+{
+    a.t[item] = (double)t;
+    bool finite = true;
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) {
+        finite = finite && isfinite(y[e]);
+        a.y[ybase + j * _numeq_ + e] = (double)y[e];
+    }
+    if (a.counters) a.counters[item] = counter;
+    if (a.newton_passes) a.newton_passes[item] = passes;
+    if (a.flags) a.flags[item] = (capped ? SODECL_FLAG_NEWTON_CAP : 0) | (finite ? 0 : SODECL_FLAG_NONFINITE);
+}
+
+#if SODECL_LANES == 1 && (SODECL_SOLVER == 3 || SODECL_SOLVER == 4)
+// Implicit solvers, one lane per orbit: Newton passes drive the loop, as in
+// the single-system kernel.  A lane whose iteration has converged commits
+// its step and starts the next at the following pass (sodecl_step_newton's
+// arithmetic, in the same order), so the lanes of a warp do not wait at
+// every step for the one that needs the most passes.  Parameters stay fixed
+// in the inner pass loop (their reciprocals stay out of it); the lanes whose
+// orbit is done take their next one from the class queue between inner
+// loops.  Called by all 32 lanes of a warp together.
+__device__ __forceinline__ void sodecl_class_run(const sodecl_batch_args &a, const int cls, double *)
+{
+    const long long begin = a.begin[cls];
+    const unsigned long long count = (unsigned long long)(a.end[cls] - begin);
+    unsigned long long *head = a.head + cls;
+    const long long ybase = a.ybase[cls], pbase = a.pbase[cls];
+
+    real_t y[_numeq_], x[_numeq_];
+    real_t p[SODECL_NPAR_ALLOC];
+    real_t t = 0;
+    long long item = -1, left = 0, passes = 0;
+    int capped = 0, pass = 0;
+    bool need = true;
+#pragma unroll 1
+    for (;;) {
+        if (need) {
+            // take orbits until one has a step to take or the queue is empty;
+            // an orbit with no step (a count of zero or less) is stored as it is
+            need = false;
+#pragma unroll 1
+            for (;;) {
+                const unsigned long long k = atomicAdd(head, 1ULL);
+                if (k >= count) {
+                    item = -1;
+                    break;
+                }
+                item = begin + (long long)k;
+                t = (real_t)a.t[item];
+#pragma unroll SODECL_EQ_UNROLL
+                for (int e = 0; e < _numeq_; ++e) y[e] = x[e] = (real_t)a.y[ybase + (long long)k * _numeq_ + e];
+#pragma unroll SODECL_PAR_UNROLL
+                for (int jj = 0; jj < _numpar_; ++jj) p[jj] = (real_t)__ldg(a.p + pbase + (long long)k * _numpar_ + jj);
+                left = a.nsteps[item];
+                passes = 0;
+                capped = pass = 0;
+                if (left > 0) break;
+                sodecl_batch_store(a, item, (long long)k, ybase, t, y, a.counters ? a.counters[item] : 0.0, 0, 0);
+            }
+        }
+        if (!__any_sync(0xffffffffu, item >= 0)) break;
+#pragma unroll 1
+        for (;;) {
+            bool finished = false;
+            if (item >= 0) {
+                // a pass limit below one takes no pass: the step is capped at once
+                const bool done = SODECL_NEWTON_MAX >= 1 && sodecl_newton_pass(_m_dt_, t, y, x, p);
+                if (SODECL_NEWTON_MAX >= 1) ++pass;
+                if (done || pass >= SODECL_NEWTON_MAX) {
+                    if (!done) capped = 1;
+                    passes += pass;
+                    pass = 0;
+                    t = t + _m_dt_;
+#pragma unroll SODECL_EQ_UNROLL
+                    for (int e = 0; e < _numeq_; ++e) y[e] = x[e];
+                    if (--left <= 0) {
+                        sodecl_batch_store(a, item, item - begin, ybase, t, y, a.counters ? a.counters[item] : 0.0,
+                                           passes, capped);
+                        item = -1;
+                        finished = true;
+                    }
+                }
+            }
+            if (__any_sync(0xffffffffu, finished)) {
+                need = finished;
+                break;
+            }
+        }
+    }
+}
+#elif SODECL_LANES == 1
 // Runs class `cls` until its queue is empty for every lane of the warp.
 // Called by all 32 lanes of a warp together.
 __device__ __forceinline__ void sodecl_class_run(const sodecl_batch_args &a, const int cls, double *)
@@ -83,17 +178,7 @@ __device__ __forceinline__ void sodecl_class_run(const sodecl_batch_args &a, con
             if (left <= 0) {
                 // store this orbit, take the next one (a count below zero
                 // takes no step, like zero)
-                const long long j = item - begin;
-                a.t[item] = (double)t;
-                bool finite = true;
-#pragma unroll SODECL_EQ_UNROLL
-                for (int e = 0; e < _numeq_; ++e) {
-                    finite = finite && isfinite(y[e]);
-                    a.y[ybase + j * _numeq_ + e] = (double)y[e];
-                }
-                if (a.counters) a.counters[item] = counter;
-                if (a.newton_passes) a.newton_passes[item] = passes;
-                if (a.flags) a.flags[item] = (capped ? SODECL_FLAG_NEWTON_CAP : 0) | (finite ? 0 : SODECL_FLAG_NONFINITE);
+                sodecl_batch_store(a, item, item - begin, ybase, t, y, counter, passes, capped);
                 passes = 0;
                 capped = 0;
                 k = atomicAdd(head, 1ULL);

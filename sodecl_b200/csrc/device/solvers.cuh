@@ -128,38 +128,10 @@ __device__ __forceinline__ void sodecl_step_euler(real_t h, real_t t, real_t *y,
 // accumulates k1 + 2 k2 + 2 k3 in place; result y + (acc + k4) h / 6.
 // x2, x3, x4 (optional) receive the stage inputs y + (h/2) k1, y + (h/2) k2,
 // y + h k3 (the adjoint reuses them).             (src/kernels/rk4.cl:17-64)
-#ifndef SODECL_RK4_ROLLED
-#define SODECL_RK4_ROLLED 0
-#endif
 __device__ __forceinline__ void sodecl_step_rk4(real_t h, real_t t, real_t *y, real_t *ynew, real_t *p,
                                                 real_t *x2 = nullptr, real_t *x3 = nullptr, real_t *x4 = nullptr)
 {
     real_t stage[_numeq_], probe[_numeq_];
-#if SODECL_RK4_ROLLED
-    // The same operations, one right-hand side in a loop over the four
-    // stages instead of four copies: a quarter of the code for the
-    // instruction cache.  Stage s evaluates at t, t + h/2, t + h/2, t + h.
-#pragma unroll SODECL_EQ_UNROLL
-    for (int e = 0; e < _numeq_; ++e) probe[e] = y[e];
-#pragma unroll 1
-    for (int s = 0; s < 4; ++s) {
-        const real_t ts = (s == 0) ? t : ((s == 3) ? t + h : t + (real_t)0.50 * h);
-        sode_system(ts, probe, stage, p);
-        if (s == 3) break;
-        const real_t hc = (s < 2) ? h * (real_t)0.50 : h;
-#pragma unroll SODECL_EQ_UNROLL
-        for (int e = 0; e < _numeq_; ++e) {
-            ynew[e] = (s == 0) ? stage[e] : ynew[e] + (real_t)2.00 * stage[e];
-            probe[e] = y[e] + hc * stage[e];
-            if (x2 && s == 0) x2[e] = probe[e];
-            if (x3 && s == 1) x3[e] = probe[e];
-            if (x4 && s == 2) x4[e] = probe[e];
-        }
-    }
-#pragma unroll SODECL_EQ_UNROLL
-    for (int e = 0; e < _numeq_; ++e)
-        ynew[e] = y[e] + (ynew[e] + stage[e]) * h / (real_t)6.00;
-#else
     sode_system(t, y, ynew, p);
 #pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) {
@@ -185,7 +157,6 @@ __device__ __forceinline__ void sodecl_step_rk4(real_t h, real_t t, real_t *y, r
 #pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e)
         ynew[e] = y[e] + (ynew[e] + stage[e]) * h / (real_t)6.00;
-#endif
 }
 
 #if SODECL_SOLVER == 3 || SODECL_SOLVER == 4

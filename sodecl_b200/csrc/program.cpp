@@ -527,13 +527,14 @@ int batch_warp_words(const std::vector<BatchClass> &classes)
 
 namespace {
 
-std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div, int block_max)
+std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div, int block_max, int min_blocks)
 {
     std::ostringstream s;
     s << "// SODECL batch program generated by libsodecl_cuda (sm_100a)\n";
     s << "#define SODECL_STEPS_ONLY 1\n#define SODECL_FP32 0\n#define SODECL_RECORD_F32 0\n";
     s << "#define SODECL_FAST_DIV " << (fast_div ? 1 : 0) << "\n";
     s << "#define SODECL_BLOCK_MAX " << block_max << "\n";
+    s << "#define SODECL_BATCH_MIN_BLOCKS " << std::max(1, min_blocks) << "\n";
     s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n" << kBatchSrc << "\n";
     static const char *per_class[] = {"SODECL_SOLVER", "SODECL_HAS_JACOBIAN", "SODECL_HAS_STOCH", "SODECL_NEWTON_MAX",
                                       "_numnoi_", "_numsteps_", "_m_dt_", "_numeq_", "_numpar_", "_epsilon1_",
@@ -574,7 +575,8 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
     }
     const int warp_words = batch_warp_words(classes);
     s << "\n#define SODECL_BATCH_WARP_WORDS " << warp_words << "\n";
-    s << "extern \"C\" __global__ void __launch_bounds__(SODECL_BLOCK_MAX) sodecl_batch(const sodecl_batch_args a)\n{\n";
+    s << "extern \"C\" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_BATCH_MIN_BLOCKS) "
+         "sodecl_batch(const sodecl_batch_args a)\n{\n";
     if (warp_words > 0) {
         s << "    extern __shared__ __align__(16) unsigned char sodecl_smem[];\n";
         s << "    double *warp_smem = reinterpret_cast<double *>(sodecl_smem) + (threadIdx.x / 32) * "
@@ -647,7 +649,7 @@ std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std:
 }
 
 std::shared_ptr<const Program> build_batch(const std::vector<BatchClass> &classes, bool fmad, bool fast_div,
-                                           int block_max)
+                                           int block_max, int min_blocks)
 {
     if (classes.empty()) throw std::runtime_error("a batch needs at least one class");
     bool fd = fast_div;
@@ -655,11 +657,11 @@ std::shared_ptr<const Program> build_batch(const std::vector<BatchClass> &classe
         if (c.system_src.find("printf") != std::string::npos) fd = false;
     if (fd) {
         try {
-            return compile_text(assemble_batch(classes, true, block_max), fmad, true, "sodecl_batch");
+            return compile_text(assemble_batch(classes, true, block_max, min_blocks), fmad, true, "sodecl_batch");
         } catch (const std::exception &) {
         }
     }
-    return compile_text(assemble_batch(classes, false, block_max), fmad, false, "sodecl_batch");
+    return compile_text(assemble_batch(classes, false, block_max, min_blocks), fmad, false, "sodecl_batch");
 }
 
 std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string &system_src)

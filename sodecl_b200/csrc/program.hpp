@@ -95,8 +95,11 @@ struct BatchClass {
 // largest (32 / lanes) x slot of the classes with lanes per orbit, else 0.
 int batch_warp_words(const std::vector<BatchClass> &classes);
 
-// All classes in one program with the persistent kernel `sodecl_batch`.
+// All classes in one program with the persistent kernel `sodecl_batch`,
+// for blocks of at most block_max threads; min_blocks > 0 asks the compiler
+// for that many resident blocks of block_max threads (a register cap of
+// 65536 / (min_blocks x block_max) per thread).
 std::shared_ptr<const Program> build_batch(const std::vector<BatchClass> &classes, bool fmad, bool fast_div,
-                                           int block_max);
+                                           int block_max, int min_blocks = 0);
 
 }  // namespace sodecl_b200

@@ -127,6 +127,7 @@ struct sodecl_ctx {
     // discrete adjoint: its own program and scratch (checkpoints, segments)
     std::shared_ptr<const Program> adj_prog;
     int adj_min_blocks = -1;
+    int adj_block = 0;
     cudaLibrary_t adj_lib = nullptr;
     cudaKernel_t adj_kernel = nullptr;
     int adj_tape = 0;
@@ -707,8 +708,13 @@ int sodecl_cuda_run(sodecl_ctx *ctx, double *out, int64_t out_len)
         }
         std::vector<int64_t> first{0};
         if (staged) {
+            // equal groups while more than two remain, then halving ones, so
+            // that the records copied after the last launch are few
             const int64_t per = std::max<int64_t>(1, (ctx->nchunks + kMinPageableGroups - 1) / kMinPageableGroups);
-            while (first.back() < ctx->nchunks) first.push_back(std::min<int64_t>(ctx->nchunks, first.back() + per));
+            while (first.back() < ctx->nchunks) {
+                const int64_t rest = ctx->nchunks - first.back();
+                first.push_back(first.back() + (rest > 2 * per ? per : std::max<int64_t>(1, (rest + 1) / 2)));
+            }
         } else {
             while (first.back() < ctx->nchunks) {
                 const int64_t rest = ctx->nchunks - first.back();
@@ -1018,29 +1024,40 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     const auto traits = sodecl_b200::inspect_system(ctx->system_src);
     // products: the file's calc_vjp, else its two Jacobians, else the tape
     const int mode = io->use_tape ? 0 : traits.has_vjp ? 2 : (traits.has_jacobian && traits.has_pjacobian) ? 1 : 0;
-    // Resident blocks the compiler must allow for (a register cap): enough
-    // that every orbit gets a thread in the first wave, up to 4 blocks of 128
-    // (128 registers).  Each thread runs its orbit's whole forward and
-    // backward sweep, so a second wave would double the time.
+    // Each thread runs its orbit's whole forward and backward sweep, so a
+    // second wave would double the time: the resident blocks the compiler
+    // must allow for (its register cap) are enough for every orbit to get a
+    // thread in the first wave, up to 512 threads per SM (128 registers) for
+    // passes with gradients and 1024 (64 registers) for the forward sweep
+    // alone, e.g. the finite-difference baseline's wide launches.  Blocks of
+    // local_group_size threads, 128 by default.  (Measured at 2^16 orbits:
+    // blocks of 32, 64 or 96 with up to 146 registers per thread run the
+    // gradient no faster than 4 blocks of 128 at 128 registers.)
+    const bool with_gradient = io->grad_params || io->grad_y0;
+    const int max_threads = with_gradient ? 512 : 1024;
     int sms = 148;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->cfg.device) != cudaSuccess) {
         cudaGetLastError();
         sms = 148;
     }
-    const long long per_wave = static_cast<long long>(std::max(1, sms)) * 128;
-    const long long waves = (io->n + per_wave - 1) / per_wave;
-    const int min_blocks = waves <= 2 ? 0 : static_cast<int>(std::min<long long>(4, waves));
+    sms = std::max(1, sms);
+    auto resident = [&](int blk) {  // blocks per SM for one wave, within max_threads
+        const long long r = (io->n + static_cast<long long>(sms) * blk - 1) / (static_cast<long long>(sms) * blk);
+        return static_cast<int>(std::max<long long>(1, std::min<long long>(r, max_threads / blk)));
+    };
+    const int block = ctx->cfg.local_group_size > 0 ? ctx->cfg.local_group_size : 128;
+    const int per_sm = resident(block);
+    const int min_blocks = per_sm * block <= 256 ? 0 : per_sm;
     // Division: loss-only passes (the forward sweep) follow the context's mode;
     // passes with gradients use IEEE division, measured faster there (the
     // reciprocal wrapper costs registers the backward sweep needs).  The
     // quotients are the same either way.
-    const bool gradient = io->grad_params || io->grad_y0;
-    const bool fast_div = !gradient && ctx->cfg.division == SODECL_DIV_RECIPROCAL;
+    const bool fast_div = !with_gradient && ctx->cfg.division == SODECL_DIV_RECIPROCAL;
     if (!ctx->adj_prog || ctx->adj_tape != tape || ctx->adj_mode != mode || ctx->adj_min_blocks != min_blocks ||
-        ctx->adj_fast_div != fast_div) {
+        ctx->adj_fast_div != fast_div || ctx->adj_block != block) {
         try {
             ProgramSpec spec = make_spec(ctx->cfg);
-            spec.block_max = 128;
+            spec.block_max = block;
             spec.min_blocks = min_blocks;
             spec.fast_div = fast_div;
             auto prog = sodecl_b200::build_adjoint(spec, ctx->system_src, tape, mode);
@@ -1052,6 +1069,7 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
             ctx->adj_mode = mode;
             ctx->adj_min_blocks = min_blocks;
             ctx->adj_fast_div = fast_div;
+            ctx->adj_block = block;
         } catch (const std::exception &ex) {
             return ctx->fail(SODECL_ERR_COMPILE, ex.what());
         }
@@ -1106,7 +1124,6 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     a.n = n;
     a.nchunks = static_cast<int>(ctx->nchunks);
     a.ckpt_every = C;
-    const int block = 128;
     void *args[] = {&a};
     SODECL_CUDA_TRY(ctx, cudaLaunchKernel(reinterpret_cast<const void *>(ctx->adj_kernel),
                                           dim3(static_cast<unsigned>((n + block - 1) / block)), dim3(block), args, 0,

@@ -266,13 +266,20 @@ def test_second_run_continues_from_device_state():
     np.testing.assert_array_equal(np.concatenate([a, b[1:]]), whole)
 
 
-def test_output_modes_agree():
+@pytest.mark.parametrize("nchunks", [0, 1, 2, 3, 10, 33])
+def test_output_modes_agree(nchunks):
+    """Pageable host memory (records staged through pinned slots by copy
+    threads, launch groups of equal then halving size), pinned host memory
+    (halving groups, copy engine), device memory (one launch) and no output
+    give the same records and final state, for record-interval counts that
+    exercise every grouping."""
     torch = pytest.importorskip("torch")
     n = 4096
     t0, y0, p = oculomotor_inputs(n, 3)
-    kw = dict(dt=1e-5, tspan=1e-3, ksteps=10, neq=6, npar=6)
+    kw = dict(dt=1e-5, tspan=nchunks * 10 * 1e-5 - 1e-9 if nchunks else 0.0, ksteps=10, neq=6, npar=6)
     outs = []
     with Integrator(system_path("oculomotor"), "rk4", orbits=n, **kw) as sim:
+        assert sim.num_chunks == nchunks
         shape = (sim.num_records, 6, n)
         sim.upload(t0, y0, p)
         outs.append(sim.run())                                     # pageable host
