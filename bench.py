@@ -284,9 +284,10 @@ def main():
     peak_tflops = peaks[a.precision]
     achieved = RK4_OPS_PER_ORBIT_STEP * n * a.nsteps / (ms * 1e-3) / 1e12 if a.solver == "rk4" else None
     # DRAM bytes per launch: ncu's dram__bytes_read.sum + dram__bytes_write.sum
-    # on a 2^18-orbit x 1000-step launch (137.3 MB, 11 records), scaled by
-    # orbits x records, which the traffic follows (it is the record stream)
-    traffic = 137.3e6 * (n * nrec) / (262144 * 11) if (a.solver == "rk4" and a.precision == "fp64") else None
+    # on a 2^18-orbit x 1000-step launch of the same kernel on the same system
+    # file (143.9 MB, 11 records), scaled by orbits x records, which the traffic
+    # follows (it is the record stream)
+    traffic = 143.9e6 * (n * nrec) / (262144 * 11) if (a.solver == "rk4" and a.precision == "fp64") else None
     algorithmic_bytes = nrec * 6 * n * 8 + n * (104 + 56)
     hbm_gbs = algorithmic_bytes / (ms * 1e-3) / 1e9
     hbm_peak = None
@@ -302,9 +303,10 @@ def main():
                 "peak_source": "measured on this GPU: FMA-chain microbenchmark (sodecl_cuda_fma_peak, fastest of "
                                "7 launches), 2 flops/FMA",
                 "ops_per_orbit_step": RK4_OPS_PER_ORBIT_STEP,
-                "fp64_pipe_active": "59.1 % of peak (ncu sm__pipe_fp64_cycles_active, 2^18-orbit x 1000-step "
-                                    "launch of this kernel); counted source ops understate the pipe work, exp and "
-                                    "division expanding to many FP64 instructions each"}
+                "fp64_pipe_active": "53.3 % of peak (ncu sm__pipe_fp64_cycles_active, 2^18-orbit x 1000-step "
+                                    "launch of this kernel on this system file, dt 1e-3); counted source ops "
+                                    "understate the pipe work, exp and division expanding to many FP64 "
+                                    "instructions each"}
 
     # ---------------- end to end through the C ABI with host buffers
     e2e = None
@@ -491,6 +493,15 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
                            "calc_jacobian_params; adjoint_tape_ms: reverse mode over sode_system"}
 
 
+def tuning_steps(steps, scale=64):
+    """Step counts for the batch tuner's trials: every orbit, each with its
+    step count divided by `scale` (at least one).  Scaling the steps and not
+    the orbits keeps the ratio of the longest orbit's time (the launch's
+    critical path) to the total work's time (throughput) that the real launch
+    has; each trial then takes about 1/scale of the launch."""
+    return np.maximum(1, steps // scale)
+
+
 def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
     """The uneven-sweep shape: orbits mixing Kuramoto N in {4, 16, 64} and the
     oculomotor model, solver per orbit in {Euler, RK4, implicit Euler}, step
@@ -501,7 +512,7 @@ def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
     One persistent launch from device work queues (autotuned launch shape,
     graph replay), against the padded alternative: one launch per class
     through the single-system kernel, every orbit of a class run for that
-    class's longest step count."""
+    class's longest step count.  Tuned as the full-size line below."""
     import torch
 
     from sodecl_b200 import Integrator, system_path
@@ -514,9 +525,7 @@ def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
     for system, solver, neq, npar, dt in classes:
         b.add_class(system_path(system), solver, neq=neq, npar=npar, dt=dt)
     b.compile()
-    sample = rng.choice(n, n // 8, replace=False)
-    b.set_items(cls[sample], np.minimum(steps[sample], 200), np.zeros(sample.size), [y0[i] for i in sample],
-                [p[i] for i in sample])
+    b.set_items(cls, tuning_steps(steps), np.zeros(n), y0, p)
     block, bps, _ = b.tune()
     b.set_items(cls, steps, np.zeros(n), y0, p)
     b.run(graph=True)  # capture
@@ -560,9 +569,9 @@ def batch_full_companion(n=1 << 18, max_steps=100000, seed=4):
     """The uneven sweep at its configured size: 2^18 orbits, step counts
     log-uniform in [10^2, 10^5] (3.8e9 orbit-steps), the same 12 classes, in
     one persistent launch (CUDA graph), after the tuner has chosen lanes per
-    class and the launch shape on an eighth of the orbits with their step
-    counts capped at 200.  One timed launch (it takes about a minute; the
-    padded comparison runs on the smaller sample above)."""
+    class, the register cap and the launch shape on every orbit with its step
+    count divided by 64 (tuning_steps).  One timed launch (it takes about a
+    minute; the padded comparison runs on the smaller sample above)."""
     from sodecl_b200 import system_path
     from sodecl_b200.batch import Batch
     from sodecl_b200.workloads import uneven_batch
@@ -572,9 +581,7 @@ def batch_full_companion(n=1 << 18, max_steps=100000, seed=4):
     for system, solver, neq, npar, dt in classes:
         b.add_class(system_path(system), solver, neq=neq, npar=npar, dt=dt)
     b.compile()
-    sample = rng.choice(n, n // 8, replace=False)
-    b.set_items(cls[sample], np.minimum(steps[sample], 200), np.zeros(sample.size), [y0[i] for i in sample],
-                [p[i] for i in sample])
+    b.set_items(cls, tuning_steps(steps), np.zeros(n), y0, p)
     block, bps, _ = b.tune()
     b.set_items(cls, steps, np.zeros(n), y0, p)
     b.set_launch(block, bps)

@@ -84,10 +84,9 @@ def _batch_main(a):
     for system, solver, neq, npar, dt in classes:
         b.add_class(system_path(system), solver, neq=neq, npar=npar, dt=dt)
     b.compile()
-    # tune on a shortened copy of an eighth of the orbits (trials advance them)
-    sample = rng.choice(a.orbits, max(1, a.orbits // 8), replace=False)
-    b.set_items(cls[sample], np.minimum(steps[sample], 200), np.zeros(sample.size), [y0[i] for i in sample],
-                [p[i] for i in sample])
+    # tune on every orbit with its step count divided by 64 (trials advance
+    # the items; the real ones are set below)
+    b.set_items(cls, np.maximum(1, steps // 64), np.zeros(a.orbits), y0, p)
     block, bps, _ = b.tune()
     for k in range(a.launches):
         b.set_items(cls, steps, np.zeros(a.orbits), y0, p)
