@@ -233,10 +233,12 @@ def main():
     assert nchunks * a.ksteps == a.nsteps, (nchunks, a.ksteps, a.nsteps)
     tuned = None
     if not a.no_tune:
-        # launch shape and division mode picked on copies of 2^17 orbits x 200
-        # steps (results are identical for every choice); outside the timing
+        # launch shape and division mode picked on copies of 2^17 orbits x 1000
+        # steps (results are identical for every choice; a thousand steps take
+        # the sample past the point where most orbits have diverged, as they
+        # have over most of the run); outside the timing
         sim.upload(t0, y0, p)
-        tuned = sim.autotune(sample_orbits=min(n, 1 << 17), sample_steps=200)
+        tuned = sim.autotune(sample_orbits=min(n, 1 << 17), sample_steps=1000)
     nrec = nchunks + 1
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream(dev)
@@ -686,7 +688,7 @@ def companions(a, n, dev, stream, peaks):
         if solver == a.solver:
             # tuned like the headline (launch shape and division mode)
             sim.upload(t0, y0, p)
-            tuned = sim.autotune(sample_orbits=min(n, 1 << 17), sample_steps=200)
+            tuned = sim.autotune(sample_orbits=min(n, 1 << 17), sample_steps=1000)
         rec = torch.empty((nrec, 6, n), dtype=torch.float64, device=dev)
         passes = torch.zeros(n, dtype=torch.int64, device=dev)
         flags = torch.zeros(n, dtype=torch.int32, device=dev)
