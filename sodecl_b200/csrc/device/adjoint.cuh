@@ -421,57 +421,12 @@ struct sodecl_adjoint_args {
     double *grad_y0;          // [n][neq] or null
     double *ckpt;             // scratch [nckpt][neq][n]
     double *ckpt_t;           // scratch [nckpt][n]
-    double *seg;              // scratch [ckpt_every][SODECL_SEG_WIDTH][n]: state, t, (RK4, two such
-                              // buffers) stage inputs
+    double *seg;              // scratch [ckpt_every][SODECL_SEG_WIDTH][n]: state, t, (RK4) stage inputs
     int *flags;               // [n] or null
     long long n;
     int nchunks;              // records - 1; steps = nchunks * _numsteps_
     int ckpt_every;           // C
 };
-
-#if SODECL_SOLVER == 2
-// Recomputation of one RK4 step from (ts, ys) into the segment slot st
-// (stride n between values): the state, t and the three stage inputs the
-// reverse step needs; then (ts, ys) <- the step's result.
-__device__ __forceinline__ void sodecl_adj_record_step(double *st, long long n, real_t &ts, real_t *ys, real_t *p)
-{
-    st[_numeq_ * n] = (double)ts;
-    for (int e = 0; e < _numeq_; ++e) st[e * n] = (double)ys[e];
-    real_t x2[_numeq_], x3[_numeq_], x4[_numeq_], ynew[_numeq_];
-    sodecl_step_rk4(_m_dt_, ts, ys, ynew, p, x2, x3, x4);
-    ts = ts + _m_dt_;
-    for (int e = 0; e < _numeq_; ++e) {
-        ys[e] = ynew[e];
-        st[(_numeq_ + 1 + e) * n] = (double)x2[e];
-        st[(2 * _numeq_ + 1 + e) * n] = (double)x3[e];
-        st[(3 * _numeq_ + 1 + e) * n] = (double)x4[e];
-    }
-}
-#endif
-
-// Reverse of step s (its record in segment slot st): first the loss term of
-// the record at state s+1, if there is one (a select, no branch: the target
-// is read either way, from record 0 when unused), then the step's adjoint.
-// ynext holds the state after step s on entry and the state before it on
-// return.
-__device__ __forceinline__ void sodecl_adj_reverse_step(const sodecl_adjoint_args &a, long long i, int s,
-                                                        const double *st, double w, const double *pd, double *ynext,
-                                                        double *lambda, double *pbar, sodecl_tape *tape, double *adj,
-                                                        int &overflow)
-{
-    const long long n = a.n;
-    const bool rec = (s + 1) % _numsteps_ == 0;
-    const long long r = rec ? (s + 1) / _numsteps_ : 0;
-    for (int e = 0; e < _numeq_; ++e) {
-        const double tg = a.targets[(r * _numeq_ + e) * n + i];
-        lambda[e] = rec ? lambda[e] + 2.0 * w * (ynext[e] - tg) : lambda[e];
-    }
-    double ystep[_numeq_], stages[SODECL_SEG_WIDTH - _numeq_ - 1 > 0 ? SODECL_SEG_WIDTH - _numeq_ - 1 : 1];
-    for (int e = 0; e < _numeq_; ++e) ystep[e] = st[e * n];
-    for (int e = 0; e < SODECL_SEG_WIDTH - _numeq_ - 1; ++e) stages[e] = st[(_numeq_ + 1 + e) * n];
-    sodecl_step_adjoint((double)_m_dt_, st[_numeq_ * n], ystep, ynext, stages, pd, lambda, pbar, tape, adj, overflow);
-    for (int e = 0; e < _numeq_; ++e) ynext[e] = ystep[e];
-}
 
 // Loss and, if grad_p is set, its gradient for every orbit.
 extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS) sodecl_adjoint(const sodecl_adjoint_args a)
@@ -530,39 +485,6 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
     double ynext[_numeq_];  // state after the step being reversed
     for (int e = 0; e < _numeq_; ++e) ynext[e] = (double)y[e];
     const int nseg = (steps + C - 1) / C;
-#if SODECL_SOLVER == 2
-    // RK4: two segment buffers.  The reverse sweep of segment sg and the
-    // recomputation of segment sg-1 (from its checkpoint, into the other
-    // buffer) run in the same loop, a step of each per iteration: two
-    // independent dependency chains in one branch-free loop body, for the
-    // scheduler to interleave.  Only the last segment can be shorter than C,
-    // so segment sg-1 is always C steps long.
-    double *const buf[2] = {a.seg + i, a.seg + (long long)C * SODECL_SEG_WIDTH * n + i};
-    const long long slot = (long long)SODECL_SEG_WIDTH * n;
-    {
-        const int sg = nseg - 1, s0 = sg * C, s1 = min(steps, s0 + C);
-        real_t ys[_numeq_];
-        real_t ts = (real_t)a.ckpt_t[(long long)sg * n + i];
-        for (int e = 0; e < _numeq_; ++e) ys[e] = (real_t)a.ckpt[((long long)sg * _numeq_ + e) * n + i];
-        for (int s = s0; s < s1; ++s) sodecl_adj_record_step(buf[sg & 1] + (s - s0) * slot, n, ts, ys, p);
-    }
-    for (int sg = nseg - 1; sg >= 1; --sg) {
-        const int s0 = sg * C, len = min(steps, s0 + C) - s0;
-        real_t ys[_numeq_];
-        real_t ts = (real_t)a.ckpt_t[(long long)(sg - 1) * n + i];
-        for (int e = 0; e < _numeq_; ++e) ys[e] = (real_t)a.ckpt[((long long)(sg - 1) * _numeq_ + e) * n + i];
-        const double *rb = buf[sg & 1];
-        double *cb = buf[(sg - 1) & 1];
-        for (int k = 0; k < len; ++k) {
-            sodecl_adj_reverse_step(a, i, s0 + len - 1 - k, rb + (len - 1 - k) * slot, w, pd, ynext, lambda, pbar,
-                                    tape, adj, overflow);
-            sodecl_adj_record_step(cb + k * slot, n, ts, ys, p);
-        }
-        for (int k = len; k < C; ++k) sodecl_adj_record_step(cb + k * slot, n, ts, ys, p);
-    }
-    for (int s = min(steps, C) - 1; s >= 0; --s)
-        sodecl_adj_reverse_step(a, i, s, buf[0] + s * slot, w, pd, ynext, lambda, pbar, tape, adj, overflow);
-#else
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int s0 = sg * C, s1 = min(steps, s0 + C);
         // recompute the segment's states from its checkpoint
@@ -573,14 +495,38 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
             double *st = a.seg + (long long)(s - s0) * SODECL_SEG_WIDTH * n + i;
             st[_numeq_ * n] = (double)ts;
             for (int e = 0; e < _numeq_; ++e) st[e * n] = (double)ys[e];
+#if SODECL_SOLVER == 2
+            // the step with its stage inputs recorded (sodecl_advance's RK4 step)
+            real_t x2[_numeq_], x3[_numeq_], x4[_numeq_], ynew[_numeq_];
+            sodecl_step_rk4(_m_dt_, ts, ys, ynew, p, x2, x3, x4);
+            ts = ts + _m_dt_;
+            for (int e = 0; e < _numeq_; ++e) {
+                ys[e] = ynew[e];
+                st[(_numeq_ + 1 + e) * n] = (double)x2[e];
+                st[(2 * _numeq_ + 1 + e) * n] = (double)x3[e];
+                st[(3 * _numeq_ + 1 + e) * n] = (double)x4[e];
+            }
+#else
             sodecl_advance(ts, ys, p, i, counter, passes, capped);
+#endif
         }
         // reverse the segment's steps
-        for (int s = s1 - 1; s >= s0; --s)
-            sodecl_adj_reverse_step(a, i, s, a.seg + (long long)(s - s0) * SODECL_SEG_WIDTH * n + i, w, pd, ynext,
-                                    lambda, pbar, tape, adj, overflow);
+        for (int s = s1 - 1; s >= s0; --s) {
+            // record at state s+1
+            if ((s + 1) % _numsteps_ == 0) {
+                const int r = (s + 1) / _numsteps_;
+                for (int e = 0; e < _numeq_; ++e)
+                    lambda[e] += 2.0 * w * (ynext[e] - a.targets[((long long)r * _numeq_ + e) * n + i]);
+            }
+            const double *st = a.seg + (long long)(s - s0) * SODECL_SEG_WIDTH * n + i;
+            double ystep[_numeq_], stages[SODECL_SEG_WIDTH - _numeq_ - 1 > 0 ? SODECL_SEG_WIDTH - _numeq_ - 1 : 1];
+            for (int e = 0; e < _numeq_; ++e) ystep[e] = st[e * n];
+            for (int e = 0; e < SODECL_SEG_WIDTH - _numeq_ - 1; ++e) stages[e] = st[(_numeq_ + 1 + e) * n];
+            sodecl_step_adjoint((double)_m_dt_, st[_numeq_ * n], ystep, ynext, stages, pd, lambda, pbar, tape, adj,
+                                overflow);
+            for (int e = 0; e < _numeq_; ++e) ynext[e] = ystep[e];
+        }
     }
-#endif
     // record 0 is the initial state
     for (int e = 0; e < _numeq_; ++e) lambda[e] += 2.0 * w * (ynext[e] - a.targets[(long long)e * n + i]);
     for (int j = 0; j < _numpar_; ++j) a.grad_p[i * _numpar_ + j] = pbar[j];

@@ -1094,11 +1094,8 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     // the segment buffer holds per step the state, t and, for RK4, the three
     // stage inputs (SODECL_SEG_WIDTH in the adjoint kernel)
     const size_t seg_width = ctx->cfg.solver == SODECL_RUNGE_KUTTA ? 4 * neq + 1 : neq + 1;
-    // RK4 recomputes one segment while it reverses the next: two buffers
-    const int64_t seg_buffers = ctx->cfg.solver == SODECL_RUNGE_KUTTA ? 2 : 1;
     const size_t need = io->grad_params || io->grad_y0
-                            ? sizeof(double) * n *
-                                  (nckpt * (neq + 1) + seg_buffers * static_cast<int64_t>(C) * seg_width)
+                            ? sizeof(double) * n * (nckpt * (neq + 1) + static_cast<int64_t>(C) * seg_width)
                             : 0;
     if (need > ctx->adj_scratch_bytes) {
         cudaFree(ctx->adj_scratch);
