@@ -233,12 +233,15 @@ def main():
     assert nchunks * a.ksteps == a.nsteps, (nchunks, a.ksteps, a.nsteps)
     tuned = None
     if not a.no_tune:
-        # launch shape and division mode picked on copies of 2^17 orbits x 1000
-        # steps (results are identical for every choice; a thousand steps take
-        # the sample past the point where most orbits have diverged, as they
-        # have over most of the run); outside the timing
+        # launch shape and division mode picked on copies of every orbit over
+        # 1000 steps (results are identical for every choice).  All the orbits,
+        # because register caps trade resident warps against spills and only
+        # a launch of many waves shows which wins (with 2^17 orbits, 64
+        # registers looked best and 85 is 3 % faster at 2^20); a thousand steps,
+        # because by then most orbits have diverged, as over most of the run.
+        # Outside the timing.
         sim.upload(t0, y0, p)
-        tuned = sim.autotune(sample_orbits=min(n, 1 << 17), sample_steps=1000)
+        tuned = sim.autotune(sample_orbits=n, sample_steps=1000)
     nrec = nchunks + 1
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream(dev)
@@ -688,7 +691,7 @@ def companions(a, n, dev, stream, peaks):
         if solver == a.solver:
             # tuned like the headline (launch shape and division mode)
             sim.upload(t0, y0, p)
-            tuned = sim.autotune(sample_orbits=min(n, 1 << 17), sample_steps=1000)
+            tuned = sim.autotune(sample_orbits=n, sample_steps=1000)
         rec = torch.empty((nrec, 6, n), dtype=torch.float64, device=dev)
         passes = torch.zeros(n, dtype=torch.int64, device=dev)
         flags = torch.zeros(n, dtype=torch.int32, device=dev)

@@ -102,8 +102,9 @@ typedef struct sodecl_cfg {
     int32_t newton_max_iter; /* implicit solvers' pass limit; default 1000 (ie.cl:69, im.cl:65) */
     int32_t record_f32;      /* device-API records stored as float (sodecl_cuda_launch only) */
     int32_t min_blocks_per_sm; /* launch-bounds occupancy hint for the compiler; 0 = default: none, except
-                                  for the implicit solvers with one thread per orbit, which are held to
-                                  128 registers a thread (1 lifts that) */
+                                  with one thread per orbit for the implicit solvers, which are held to
+                                  128 registers a thread, and for FP64 RK4 on up to 8 equations, held
+                                  to 85 (1 lifts either) */
     int32_t division;        /* FP64 quotients: SODECL_DIV_RECIPROCAL (default) or SODECL_DIV_IEEE;
                                 both give the IEEE-rounded quotient bit for bit */
     int32_t lanes_per_orbit; /* 0 or 1 (default): one thread per orbit.  2, 4, 8, 16 or 32:

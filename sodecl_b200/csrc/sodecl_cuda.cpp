@@ -433,6 +433,14 @@ ProgramSpec make_spec(const sodecl_cfg &c)
     if (spec.min_blocks == 0 && lanes_of(c) == 1 &&
         (c.solver == SODECL_IMPLICIT_EULER || c.solver == SODECL_IMPLICIT_MIDPOINT))
         spec.min_blocks = std::max(1, 65536 / (spec.block_max * 128));
+    // FP64 RK4 on small systems, one thread per orbit: by default at most 85
+    // registers a thread (three blocks of 256).  Measured on the oculomotor
+    // model at 2^20 orbits x 10^4 steps: 397 ms against 426 ms with no cap
+    // and 411 ms at 64 registers (the reference's system file; the package's
+    // 362 / 381 / 371 ms).
+    if (spec.min_blocks == 0 && lanes_of(c) == 1 && c.solver == SODECL_RUNGE_KUTTA && !spec.fp32 &&
+        c.num_equat <= 8)
+        spec.min_blocks = std::max(1, 65536 / (spec.block_max * 85));
     spec.fast_div = c.division == SODECL_DIV_RECIPROCAL;
     spec.lanes = lanes_of(c);
     spec.rtol = c.rtol;
@@ -896,8 +904,10 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
     // lanes per orbit: up to the first power of two >= the equations
     const auto traits = sodecl_b200::inspect_system(ctx->system_src);
     const int solver = ctx->cfg.solver;
-    // implicit solvers run under a register cap by default (min_blocks 0); 1 lifts it
-    if (solver == SODECL_IMPLICIT_EULER || solver == SODECL_IMPLICIT_MIDPOINT)
+    // implicit solvers and FP64 RK4 on small systems run under a register cap
+    // by default (min_blocks 0); 1 lifts it
+    if (solver == SODECL_IMPLICIT_EULER || solver == SODECL_IMPLICIT_MIDPOINT ||
+        (solver == SODECL_RUNGE_KUTTA && ctx->cfg.precision == SODECL_FP64 && ctx->cfg.num_equat <= 8))
         cands.push_back({128, 1, ctx->cfg.precision == SODECL_FP64 ? SODECL_DIV_RECIPROCAL : SODECL_DIV_IEEE, 1});
     const bool row_ok = lanes_supported(traits, solver);
     if (row_ok) {
