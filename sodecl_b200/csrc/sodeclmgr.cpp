@@ -121,6 +121,15 @@ int sodeclmgr::setup_sode_solver()
         std::cout << "Failed to build kernel." << std::endl << m_error << std::endl;
         return 0;
     }
+    {
+        // the assembled program, written to the working directory as the
+        // reference writes its OpenCL source (src/sodeclmgr.cpp:497-500)
+        std::string program(sodecl_cuda_program_source(m_ctx, nullptr, 0) + 1, '\0');
+        sodecl_cuda_program_source(m_ctx, &program[0], program.size());
+        program.resize(program.size() - 1);
+        std::ofstream dump("Generated_kernel.cl");
+        dump << program;
+    }
     rc = sodecl_cuda_upload(m_ctx, m_t0, m_y0, m_params, m_counters);
     if (rc != SODECL_OK) {
         m_error = ctx_error(m_ctx);

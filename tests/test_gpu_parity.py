@@ -352,6 +352,10 @@ def test_cpp_sodeclmgr_drop_in(tmp_path):
     assert np.isclose(res, golden).all()
     filemode = np.fromfile(str(tmp_path / "sodecloutput.bin"))
     np.testing.assert_array_equal(filemode, np.fromfile(out_file))
+    # the assembled program in the working directory, as the reference leaves
+    # its OpenCL source there (src/sodeclmgr.cpp:497-500)
+    dumped = (tmp_path / "Generated_kernel.cl").read_text()
+    assert "#define _m_dt_" in dumped and "sode_system" in dumped and "sodecl_orbits" in dumped
 
 
 @pytest.mark.parametrize("solver", ["ie", "im"])
