@@ -290,9 +290,9 @@ def main():
     achieved = RK4_OPS_PER_ORBIT_STEP * n * a.nsteps / (ms * 1e-3) / 1e12 if a.solver == "rk4" else None
     # DRAM bytes per launch: ncu's dram__bytes_read.sum + dram__bytes_write.sum
     # on a 2^18-orbit x 1000-step launch of the same kernel on the same system
-    # file (143.9 MB, 11 records), scaled by orbits x records, which the traffic
-    # follows (it is the record stream)
-    traffic = 143.9e6 * (n * nrec) / (262144 * 11) if (a.solver == "rk4" and a.precision == "fp64") else None
+    # file with the default 85-register cap (129.2 MB, 11 records), scaled by
+    # orbits x records, which the traffic follows (it is the record stream)
+    traffic = 129.2e6 * (n * nrec) / (262144 * 11) if (a.solver == "rk4" and a.precision == "fp64") else None
     algorithmic_bytes = nrec * 6 * n * 8 + n * (104 + 56)
     hbm_gbs = algorithmic_bytes / (ms * 1e-3) / 1e9
     hbm_peak = None
@@ -308,7 +308,7 @@ def main():
                 "peak_source": "measured on this GPU: FMA-chain microbenchmark (sodecl_cuda_fma_peak, fastest of "
                                "7 launches), 2 flops/FMA",
                 "ops_per_orbit_step": RK4_OPS_PER_ORBIT_STEP,
-                "fp64_pipe_active": "53.3 % of peak (ncu sm__pipe_fp64_cycles_active, 2^18-orbit x 1000-step "
+                "fp64_pipe_active": "52.4 % of peak (ncu sm__pipe_fp64_cycles_active, 2^18-orbit x 1000-step "
                                     "launch of this kernel on this system file, dt 1e-3); counted source ops "
                                     "understate the pipe work, exp and division expanding to many FP64 "
                                     "instructions each"}
