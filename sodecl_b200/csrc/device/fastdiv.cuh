@@ -4,11 +4,6 @@
 #ifndef SODECL_FASTDIV_CUH
 #define SODECL_FASTDIV_CUH
 
-// The IEEE quotient, out of line: the rare operands that leave the
-// reciprocal's range call it, and every quotient site of a system file keeps
-// only the call, not a copy of the division's code (instruction cache).
-__device__ __noinline__ double sodecl_div_ieee(double a, double b) { return a / b; }
-
 // ---------------------------------------------------------------------------
 // q = a*r, e = fma(-q, b, a), q' = fma(e, r, q) with r = RN(1/b) gives the
 // correctly rounded a/b (Markstein, "Computation of elementary functions on
@@ -38,7 +33,7 @@ __device__ __forceinline__ double sodecl_div_by(double a, double b, double r)
     // special-case path, which orbits that have diverged would take every step
     if (a != a || b != b)
         return a + b;
-    return sodecl_div_ieee(a, b);
+    return a / b;
 }
 
 __device__ __forceinline__ double sodecl_div_rcp(double a, double b) { return sodecl_div_by(a, b, 1.0 / b); }
