@@ -86,8 +86,6 @@ constexpr int kMinPageableGroups = 16;
 // every context; one run at a time copies through them.
 constexpr int kStageWorkers = 8;
 constexpr size_t kStageSlotBytes = size_t(8) << 20;
-// Uploads of pageable inputs at least this large are staged the same way.
-constexpr size_t kStagedUploadBytes = size_t(32) << 20;
 
 struct StagingPool {
     std::mutex in_use;
@@ -302,69 +300,6 @@ cudaError_t staged_copy(int device, double *out, const double *d_rec, const std:
     for (int w = 0; w < nworkers; ++w) threads.emplace_back(work, w);
     for (auto &t : threads) t.join();
     return static_cast<cudaError_t>(first_error.load());
-}
-
-// A piece of an upload: `count` doubles from pageable host memory to device
-// memory.
-struct UpPiece {
-    const double *src;
-    double *dst;
-    int64_t count;
-};
-
-// Uploads the pieces through the pinned staging pool (the counterpart of
-// staged_copy): worker w takes pieces w, w + W, ...; it copies each into one
-// of its two slots on the host and queues the slot's copy to the device on
-// its own stream, waiting for a slot's previous copy before refilling it.
-// `pool` is locked by the caller.  Returns when every copy has finished.
-cudaError_t staged_upload(int device, const std::vector<UpPiece> &pieces, StagingPool &pool)
-{
-    const int nworkers = static_cast<int>(pool.slots.size() / 2);
-    std::atomic<int> first_error{static_cast<int>(cudaSuccess)};
-    auto note = [&](cudaError_t e) {
-        if (e != cudaSuccess) {
-            int expected = static_cast<int>(cudaSuccess);
-            first_error.compare_exchange_strong(expected, static_cast<int>(e));
-        }
-        return e == cudaSuccess;
-    };
-    auto work = [&](int w) {
-        if (!note(cudaSetDevice(device))) return;
-        cudaStream_t st = nullptr;
-        cudaEvent_t ev[2] = {nullptr, nullptr};
-        if (!note(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking))) return;
-        bool ok = note(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming)) &&
-                  note(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
-        int k = 0;
-        for (size_t j = static_cast<size_t>(w); ok && j < pieces.size(); j += nworkers, ++k) {
-            const int slot = k & 1;
-            if (k >= 2 && !note(cudaEventSynchronize(ev[slot]))) break;  // the slot's previous copy
-            if (first_error.load() != static_cast<int>(cudaSuccess)) break;
-            const size_t bytes = static_cast<size_t>(pieces[j].count) * sizeof(double);
-            std::memcpy(pool.slots[2 * w + slot], pieces[j].src, bytes);
-            ok = note(cudaMemcpyAsync(pieces[j].dst, pool.slots[2 * w + slot], bytes, cudaMemcpyHostToDevice, st)) &&
-                 note(cudaEventRecord(ev[slot], st));
-        }
-        note(cudaStreamSynchronize(st));
-        for (auto e : ev)
-            if (e) cudaEventDestroy(e);
-        cudaStreamDestroy(st);
-    };
-    std::vector<std::thread> threads;
-    threads.reserve(nworkers);
-    for (int w = 0; w < nworkers; ++w) threads.emplace_back(work, w);
-    for (auto &t : threads) t.join();
-    return static_cast<cudaError_t>(first_error.load());
-}
-
-bool host_pageable(const void *p)
-{
-    cudaPointerAttributes attr{};
-    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
-        cudaGetLastError();
-        return true;
-    }
-    return attr.type == cudaMemoryTypeUnregistered;
 }
 
 // Pins the staging pool's slots on first use; false if pinned memory is not
@@ -657,36 +592,10 @@ int sodecl_cuda_upload(sodecl_ctx *ctx, const double *t0, const double *y0, cons
         SODECL_CUDA_TRY(ctx, cudaMalloc(&ctx->d_passes, n * sizeof(long long)));
         SODECL_CUDA_TRY(ctx, cudaMalloc(&ctx->d_flags, n * sizeof(int)));
     }
-    // Large pageable inputs go through the pinned staging pool (several host
-    // threads, several streams); others with one copy each.
-    bool staged = false;
-    if ((n * (1 + neq + npar)) * sizeof(double) >= kStagedUploadBytes && host_pageable(t0) && host_pageable(y0) &&
-        (npar == 0 || host_pageable(params))) {
-        StagingPool &pool = staging_pool();
-        std::lock_guard<std::mutex> lock(pool.in_use);
-        if (staging_ready(pool)) {
-            SODECL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-            const int64_t slot_elems = static_cast<int64_t>(kStageSlotBytes / sizeof(double));
-            std::vector<UpPiece> pieces;
-            auto add = [&](const double *src, double *dst, int64_t count) {
-                for (int64_t e = 0; e < count; e += slot_elems)
-                    pieces.push_back(UpPiece{src + e, dst + e, std::min(slot_elems, count - e)});
-            };
-            add(t0, ctx->d_t, static_cast<int64_t>(n));
-            add(y0, ctx->d_y, static_cast<int64_t>(n * neq));
-            if (npar > 0) add(params, ctx->d_p, static_cast<int64_t>(n * npar));
-            const cudaError_t e = staged_upload(ctx->cfg.device, pieces, pool);
-            if (e != cudaSuccess) return cuda_fail(ctx, e, "staged upload");
-            staged = true;
-        }
-    }
-    if (!staged) {
-        SODECL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_t, t0, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-        SODECL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_y, y0, n * neq * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-        if (npar > 0)
-            SODECL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_p, params, n * npar * sizeof(double), cudaMemcpyHostToDevice,
-                                                 ctx->stream));
-    }
+    SODECL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_t, t0, n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    SODECL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_y, y0, n * neq * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    if (npar > 0)
+        SODECL_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->d_p, params, n * npar * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     std::vector<double> drawn;
     if (ctx->cfg.solver == SODECL_DORMAND_PRINCE && counters) {
         // each orbit's next step size
