@@ -64,15 +64,19 @@ extern "C" {
 #define SODECL_FP64 0
 #define SODECL_FP32 1
 
-/* how FP64 programs divide: SODECL_DIV_RECIPROCAL (default) computes a/b as
- * a*r plus two FMA corrections with r = 1/b (hoistable out of the step loop for
- * parameters and constants), returns NaN at once for a NaN operand, and falls
- * back to IEEE division outside [2^-500, 2^500): the same quotient as
- * SODECL_DIV_IEEE bit for bit (NaN payloads aside).  On the oculomotor RK4
- * workload it is 2 % faster on converging orbits and 1.8x on diverged ones;
- * sodecl_cuda_autotune measures it for a given system file. */
+/* how programs divide: SODECL_DIV_RECIPROCAL computes a/b as a*r plus two FMA
+ * corrections with r = 1/b (hoistable out of the step loop for parameters and
+ * constants), returns NaN at once for a NaN operand, and falls back to IEEE
+ * division outside [2^-500, 2^500) (FP32: [2^-60, 2^60)): the same quotient as
+ * SODECL_DIV_IEEE bit for bit (NaN payloads aside).  SODECL_DIV_DEFAULT (what
+ * sodecl_cfg_init sets) is the reciprocal form in FP64 and IEEE division in
+ * FP32.  On the oculomotor RK4 workload in FP64 the reciprocal form is 2 %
+ * faster on converging orbits and 1.8x on diverged ones; in FP32 it gains on
+ * diverged orbits and loses on converging ones.  sodecl_cuda_autotune measures
+ * both for a given system file. */
 #define SODECL_DIV_RECIPROCAL 0
 #define SODECL_DIV_IEEE 1
+#define SODECL_DIV_DEFAULT 2
 
 /* per-orbit status flags (sodecl_cuda_status) */
 #define SODECL_FLAG_NEWTON_CAP 1   /* some implicit step stopped at newton_max_iter, or an
@@ -105,7 +109,8 @@ typedef struct sodecl_cfg {
                                   with one thread per orbit for the implicit solvers, which are held to
                                   128 registers a thread, and for FP64 RK4 on up to 8 equations, held
                                   to 85 (1 lifts either) */
-    int32_t division;        /* FP64 quotients: SODECL_DIV_RECIPROCAL (default) or SODECL_DIV_IEEE;
+    int32_t division;        /* quotients: SODECL_DIV_DEFAULT (the default: reciprocal in FP64, IEEE in
+                                FP32), SODECL_DIV_RECIPROCAL or SODECL_DIV_IEEE;
                                 both give the IEEE-rounded quotient bit for bit */
     int32_t lanes_per_orbit; /* 0 or 1 (default): one thread per orbit.  2, 4, 8, 16 or 32:
                                 that many lanes of a warp share an orbit, each evaluating
@@ -264,7 +269,7 @@ int sodecl_cuda_kernel_info(sodecl_ctx *ctx, int *regs, int *local_bytes, int *m
 
 /* Autotuner: times candidate launch shapes (threads per block, resident-block
  * hints, and lanes per orbit when the system file has sode_system_row and the
- * solver is explicit or stochastic) and FP64 division modes on copies of the
+ * solver is explicit or stochastic) and division modes on copies of the
  * first `sample_orbits` uploaded orbits for `sample_steps` steps -- the
  * context's state does not advance -- and rebuilds the program with the
  * fastest.  All candidates give identical results.  Writes the choice (any
@@ -402,6 +407,11 @@ int sodecl_cuda_noise_stream(int device, const int64_t *gids, const double *coun
  * differing pair. */
 int sodecl_cuda_division_check(int device, int64_t pairs, uint64_t seed, int64_t *mismatches, double *first_a,
                                double *first_b);
+
+/* The same for FP32 programs' reciprocal quotient (binary32, fast path for
+ * |a|, |b| in [2^-60, 2^60)) against IEEE float division. */
+int sodecl_cuda_division_check_f32(int device, int64_t pairs, uint64_t seed, int64_t *mismatches, float *first_a,
+                                   float *first_b);
 
 /* Issue-rate microbenchmark of the FP64 (precision 0) or FP32 (1) FMA pipe:
  * independent FMA chains on every SM, timed with CUDA events, the fastest

@@ -26,7 +26,7 @@ ERR_UNSUPPORTED = -9
 ABI_VERSION = 3
 STOCHASTIC_EULER, EULER, RUNGE_KUTTA, IMPLICIT_EULER, IMPLICIT_MIDPOINT, DORMAND_PRINCE = range(6)
 FP64, FP32 = 0, 1
-DIV_RECIPROCAL, DIV_IEEE = 0, 1
+DIV_RECIPROCAL, DIV_IEEE, DIV_DEFAULT = 0, 1, 2
 FLAG_NEWTON_CAP = 1
 FLAG_NONFINITE = 2
 
@@ -152,6 +152,8 @@ SIGNATURES = {
                                            C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     "sodecl_cuda_division_check": (C.c_int, [C.c_int, C.c_int64, C.c_uint64, C.POINTER(C.c_int64),
                                              C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "sodecl_cuda_division_check_f32": (C.c_int, [C.c_int, C.c_int64, C.c_uint64, C.POINTER(C.c_int64),
+                                                 C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "sodecl_class_cfg_init": (None, [C.POINTER(ClassCfg)]),
     "sodecl_batch_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(_P)]),
     "sodecl_batch_add_class": (C.c_int, [_P, C.c_char_p, C.c_size_t, C.POINTER(ClassCfg), C.POINTER(C.c_int32)]),

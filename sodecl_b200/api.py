@@ -50,7 +50,7 @@ class Integrator:
 
     def __init__(self, system, solver, *, dt, tspan, ksteps, neq, npar, orbits, nnoi=0, device=0,
                  precision="fp64", fmad=True, newton_tol=1e-7, newton_max_iter=1000, block=0,
-                 record_f32=False, min_blocks=0, division="reciprocal", lanes=1, system_src=None, rtol=1e-6,
+                 record_f32=False, min_blocks=0, division="default", lanes=1, system_src=None, rtol=1e-6,
                  atol=1e-9, max_steps=100000):
         cfg = N.Cfg()
         N.lib.sodecl_cfg_init(C.byref(cfg))
@@ -70,7 +70,10 @@ class Integrator:
         cfg.newton_max_iter = int(newton_max_iter)
         cfg.record_f32 = 1 if record_f32 else 0
         cfg.min_blocks_per_sm = int(min_blocks)
-        cfg.division = N.DIV_RECIPROCAL if str(division).lower() == "reciprocal" else N.DIV_IEEE
+        modes = {"default": N.DIV_DEFAULT, "reciprocal": N.DIV_RECIPROCAL, "ieee": N.DIV_IEEE}
+        if str(division).lower() not in modes:
+            raise ValueError("division must be 'default', 'reciprocal' or 'ieee', not %r" % (division,))
+        cfg.division = modes[str(division).lower()]
         cfg.lanes_per_orbit = int(lanes)
         cfg.rtol = float(rtol)
         cfg.atol = float(atol)

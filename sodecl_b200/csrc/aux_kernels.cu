@@ -103,6 +103,47 @@ __global__ void division_check_kernel(unsigned long long seed, long long per_thr
     (void)bad;
 }
 
+// The same for binary32: random patterns with exponents within +-70 of 1 (the
+// fast path and both sides of its bounds), significands near 1 and 2,
+// anything, and specials.
+__device__ __forceinline__ float division_operand_f32(unsigned long long &state)
+{
+    const unsigned long long u = splitmix64(state);
+    const unsigned kind = (unsigned)(u >> 60);
+    unsigned bits = (unsigned)splitmix64(state);
+    if (kind < 8) {
+        const unsigned e = 127 - 70 + (unsigned)(u % 140);
+        bits = (bits & 0x807FFFFFu) | (e << 23);
+    } else if (kind < 11) {
+        const unsigned e = 127 - 20 + (unsigned)(u % 40);
+        const unsigned k = (unsigned)((u >> 20) & 63);
+        const unsigned m = ((u >> 30) & 1) ? k : (0x007FFFFFu - k);
+        bits = (bits & 0x80000000u) | (e << 23) | m;
+    } else if (kind < 15) {
+        // anything: full exponent range, subnormals, Inf, NaN
+    } else {
+        const float special[8] = {0.0f, -0.0f, 1.0f / 0.0f, -1.0f / 0.0f, 1.4e-45f, 1.17549435e-38f, 3.40282347e38f,
+                                  6.0f};
+        return special[u & 7];
+    }
+    return __int_as_float((int)bits);
+}
+
+__global__ void division_check_f32_kernel(unsigned long long seed, long long per_thread, unsigned long long *mismatches,
+                                          float *first)
+{
+    unsigned long long state = seed ^ (0xD1B54A32D192ED03ULL * (blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x + 1));
+    for (long long i = 0; i < per_thread; ++i) {
+        const float a = division_operand_f32(state), b = division_operand_f32(state);
+        const float want = a / b, got = sodecl_div_rcp(a, b);
+        const bool same = (__float_as_int(want) == __float_as_int(got)) || (want != want && got != got);
+        if (!same && atomicAdd(mismatches, 1ULL) == 0) {
+            first[0] = a;
+            first[1] = b;
+        }
+    }
+}
+
 // Eight independent FMA chains per thread, unrolled; every SM full of warps.
 template <class T>
 __global__ void __launch_bounds__(256) fma_chains_kernel(T *sink, int iters, T a, T b)
@@ -234,6 +275,42 @@ extern "C" int sodecl_cuda_division_check(int device, int64_t pairs, uint64_t se
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) rc = SODECL_ERR_CUDA;
     unsigned long long bad = 0;
     double first[2] = {0.0, 0.0};
+    if (rc == SODECL_OK) {
+        cudaMemcpy(&bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost);
+        cudaMemcpy(first, d_first, sizeof(first), cudaMemcpyDeviceToHost);
+    }
+    cudaFree(d_bad);
+    cudaFree(d_first);
+    *mismatches = (int64_t)bad;
+    if (first_a) *first_a = first[0];
+    if (first_b) *first_b = first[1];
+    return rc;
+}
+
+extern "C" int sodecl_cuda_division_check_f32(int device, int64_t pairs, uint64_t seed, int64_t *mismatches,
+                                              float *first_a, float *first_b)
+{
+    if (pairs < 1 || !mismatches) return SODECL_ERR_INVALID_ARG;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) { cudaGetLastError(); return SODECL_ERR_NO_DEVICE; }
+    DeviceGuard guard(device);
+    const int block = 256, blocks = 148 * 8;
+    const long long per_thread = (pairs + (long long)block * blocks - 1) / ((long long)block * blocks);
+    unsigned long long *d_bad = nullptr;
+    float *d_first = nullptr;
+    if (cudaMalloc(&d_bad, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&d_first, 2 * sizeof(float)) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(d_bad);
+        return SODECL_ERR_OUT_OF_MEMORY;
+    }
+    int rc = SODECL_OK;
+    cudaMemset(d_bad, 0, sizeof(unsigned long long));
+    cudaMemset(d_first, 0, 2 * sizeof(float));
+    division_check_f32_kernel<<<blocks, block>>>(seed, per_thread, d_bad, d_first);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) rc = SODECL_ERR_CUDA;
+    unsigned long long bad = 0;
+    float first[2] = {0.0f, 0.0f};
     if (rc == SODECL_OK) {
         cudaMemcpy(&bad, d_bad, sizeof(bad), cudaMemcpyDeviceToHost);
         cudaMemcpy(first, d_first, sizeof(first), cudaMemcpyDeviceToHost);

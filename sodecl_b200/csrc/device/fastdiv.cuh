@@ -38,4 +38,23 @@ __device__ __forceinline__ double sodecl_div_by(double a, double b, double r)
 
 __device__ __forceinline__ double sodecl_div_rcp(double a, double b) { return sodecl_div_by(a, b, 1.0 / b); }
 
+// The same in binary32, with the range [2^-60, 2^60) for |a| and |b|: there
+// r, q, the product q*b and the residual stay normal floats, so the residual is
+// exact and q' the correctly rounded quotient.
+__device__ __forceinline__ float sodecl_div_by(float a, float b, float r)
+{
+    const float q = a * r;
+    const float e = __fmaf_rn(-q, b, a);
+    const float q2 = __fmaf_rn(e, r, q);
+    const unsigned ea = ((unsigned)__float_as_int(a) >> 23) & 0xffu;
+    const unsigned eb = ((unsigned)__float_as_int(b) >> 23) & 0xffu;
+    if ((ea - 67u) < 120u && (eb - 67u) < 120u)
+        return q2;
+    if (a != a || b != b)
+        return a + b;
+    return a / b;
+}
+
+__device__ __forceinline__ float sodecl_div_rcp(float a, float b) { return sodecl_div_by(a, b, 1.0f / b); }
+
 #endif

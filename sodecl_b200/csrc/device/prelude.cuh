@@ -15,78 +15,84 @@ typedef unsigned long long sodecl_u64;
 typedef long long sodecl_i64;
 
 #if SODECL_FAST_DIV
-// A double with the quotient above as its `/`.  Every other operation is the
-// plain double operation (so FMA contraction and results are unchanged).
-// Conversions out of it are explicit, so mixed expressions stay unambiguous;
-// a system file that needs an implicit conversion fails to compile with it
-// and the front end builds the plain-double program instead.
-struct sodecl_f64 {
-    double v;
-    __device__ __forceinline__ sodecl_f64() = default;
-    __device__ __forceinline__ constexpr sodecl_f64(double x) : v(x) {}
-    __device__ __forceinline__ constexpr sodecl_f64(float x) : v(x) {}
-    __device__ __forceinline__ constexpr sodecl_f64(int x) : v(x) {}
-    __device__ __forceinline__ constexpr sodecl_f64(unsigned x) : v(x) {}
-    __device__ __forceinline__ constexpr sodecl_f64(long x) : v((double)x) {}
-    __device__ __forceinline__ constexpr sodecl_f64(long long x) : v((double)x) {}
-    __device__ __forceinline__ constexpr sodecl_f64(unsigned long x) : v((double)x) {}
-    __device__ __forceinline__ constexpr sodecl_f64(unsigned long long x) : v((double)x) {}
-    __device__ __forceinline__ explicit operator double() const { return v; }
+#if SODECL_FP32
+typedef float sodecl_num_t;
+#else
+typedef double sodecl_num_t;
+#endif
+// A double (a float in FP32 programs) with the quotient above as its `/`.
+// Every other operation is the plain operation on the scalar (so FMA
+// contraction and results are unchanged).  Conversions out of it are
+// explicit, so mixed expressions stay unambiguous; a system file that needs an
+// implicit conversion fails to compile with it and the front end builds the
+// plain program instead.
+struct sodecl_num {
+    sodecl_num_t v;
+    __device__ __forceinline__ sodecl_num() = default;
+    __device__ __forceinline__ constexpr sodecl_num(double x) : v((sodecl_num_t)x) {}
+    __device__ __forceinline__ constexpr sodecl_num(float x) : v((sodecl_num_t)x) {}
+    __device__ __forceinline__ constexpr sodecl_num(int x) : v((sodecl_num_t)x) {}
+    __device__ __forceinline__ constexpr sodecl_num(unsigned x) : v((sodecl_num_t)x) {}
+    __device__ __forceinline__ constexpr sodecl_num(long x) : v((sodecl_num_t)x) {}
+    __device__ __forceinline__ constexpr sodecl_num(long long x) : v((sodecl_num_t)x) {}
+    __device__ __forceinline__ constexpr sodecl_num(unsigned long x) : v((sodecl_num_t)x) {}
+    __device__ __forceinline__ constexpr sodecl_num(unsigned long long x) : v((sodecl_num_t)x) {}
+    __device__ __forceinline__ explicit operator double() const { return (double)v; }
     __device__ __forceinline__ explicit operator float() const { return (float)v; }
     __device__ __forceinline__ explicit operator int() const { return (int)v; }
     __device__ __forceinline__ explicit operator unsigned() const { return (unsigned)v; }
     __device__ __forceinline__ explicit operator long() const { return (long)v; }
     __device__ __forceinline__ explicit operator long long() const { return (long long)v; }
     __device__ __forceinline__ explicit operator unsigned long long() const { return (unsigned long long)v; }
-    __device__ __forceinline__ explicit operator bool() const { return v != 0.0; }
-    __device__ __forceinline__ sodecl_f64 &operator+=(sodecl_f64 o) { v = v + o.v; return *this; }
-    __device__ __forceinline__ sodecl_f64 &operator-=(sodecl_f64 o) { v = v - o.v; return *this; }
-    __device__ __forceinline__ sodecl_f64 &operator*=(sodecl_f64 o) { v = v * o.v; return *this; }
-    __device__ __forceinline__ sodecl_f64 &operator/=(sodecl_f64 o) { v = sodecl_div_rcp(v, o.v); return *this; }
-    __device__ __forceinline__ sodecl_f64 &operator++() { v = v + 1.0; return *this; }
-    __device__ __forceinline__ sodecl_f64 &operator--() { v = v - 1.0; return *this; }
+    __device__ __forceinline__ explicit operator bool() const { return v != (sodecl_num_t)0; }
+    __device__ __forceinline__ sodecl_num &operator+=(sodecl_num o) { v = v + o.v; return *this; }
+    __device__ __forceinline__ sodecl_num &operator-=(sodecl_num o) { v = v - o.v; return *this; }
+    __device__ __forceinline__ sodecl_num &operator*=(sodecl_num o) { v = v * o.v; return *this; }
+    __device__ __forceinline__ sodecl_num &operator/=(sodecl_num o) { v = sodecl_div_rcp(v, o.v); return *this; }
+    __device__ __forceinline__ sodecl_num &operator++() { v = v + (sodecl_num_t)1; return *this; }
+    __device__ __forceinline__ sodecl_num &operator--() { v = v - (sodecl_num_t)1; return *this; }
 };
-__device__ __forceinline__ sodecl_f64 operator+(sodecl_f64 a) { return a; }
-__device__ __forceinline__ sodecl_f64 operator-(sodecl_f64 a) { return sodecl_f64(-a.v); }
-__device__ __forceinline__ sodecl_f64 operator+(sodecl_f64 a, sodecl_f64 b) { return sodecl_f64(a.v + b.v); }
-__device__ __forceinline__ sodecl_f64 operator-(sodecl_f64 a, sodecl_f64 b) { return sodecl_f64(a.v - b.v); }
-__device__ __forceinline__ sodecl_f64 operator*(sodecl_f64 a, sodecl_f64 b) { return sodecl_f64(a.v * b.v); }
-__device__ __forceinline__ sodecl_f64 operator/(sodecl_f64 a, sodecl_f64 b) { return sodecl_f64(sodecl_div_rcp(a.v, b.v)); }
-__device__ __forceinline__ bool operator<(sodecl_f64 a, sodecl_f64 b) { return a.v < b.v; }
-__device__ __forceinline__ bool operator>(sodecl_f64 a, sodecl_f64 b) { return a.v > b.v; }
-__device__ __forceinline__ bool operator<=(sodecl_f64 a, sodecl_f64 b) { return a.v <= b.v; }
-__device__ __forceinline__ bool operator>=(sodecl_f64 a, sodecl_f64 b) { return a.v >= b.v; }
-__device__ __forceinline__ bool operator==(sodecl_f64 a, sodecl_f64 b) { return a.v == b.v; }
-__device__ __forceinline__ bool operator!=(sodecl_f64 a, sodecl_f64 b) { return a.v != b.v; }
-#define SODECL_F64_UNARY(fn) \
-    __device__ __forceinline__ sodecl_f64 fn(sodecl_f64 a) { return sodecl_f64(::fn(a.v)); }
-SODECL_F64_UNARY(exp) SODECL_F64_UNARY(exp2) SODECL_F64_UNARY(expm1) SODECL_F64_UNARY(log)
-SODECL_F64_UNARY(log2) SODECL_F64_UNARY(log10) SODECL_F64_UNARY(log1p) SODECL_F64_UNARY(sqrt)
-SODECL_F64_UNARY(rsqrt) SODECL_F64_UNARY(cbrt) SODECL_F64_UNARY(sin) SODECL_F64_UNARY(cos)
-SODECL_F64_UNARY(tan) SODECL_F64_UNARY(asin) SODECL_F64_UNARY(acos) SODECL_F64_UNARY(atan)
-SODECL_F64_UNARY(sinh) SODECL_F64_UNARY(cosh) SODECL_F64_UNARY(tanh) SODECL_F64_UNARY(asinh)
-SODECL_F64_UNARY(acosh) SODECL_F64_UNARY(atanh) SODECL_F64_UNARY(fabs) SODECL_F64_UNARY(floor)
-SODECL_F64_UNARY(ceil) SODECL_F64_UNARY(trunc) SODECL_F64_UNARY(round) SODECL_F64_UNARY(rint)
-SODECL_F64_UNARY(erf) SODECL_F64_UNARY(erfc) SODECL_F64_UNARY(tgamma) SODECL_F64_UNARY(lgamma)
-#define SODECL_F64_BINARY(fn) \
-    __device__ __forceinline__ sodecl_f64 fn(sodecl_f64 a, sodecl_f64 b) { return sodecl_f64(::fn(a.v, b.v)); }
-SODECL_F64_BINARY(pow) SODECL_F64_BINARY(fmin) SODECL_F64_BINARY(fmax) SODECL_F64_BINARY(fmod)
-SODECL_F64_BINARY(atan2) SODECL_F64_BINARY(hypot) SODECL_F64_BINARY(copysign) SODECL_F64_BINARY(fdim)
-SODECL_F64_BINARY(remainder)
-__device__ __forceinline__ sodecl_f64 fma(sodecl_f64 a, sodecl_f64 b, sodecl_f64 c) { return sodecl_f64(::fma(a.v, b.v, c.v)); }
-__device__ __forceinline__ sodecl_f64 abs(sodecl_f64 a) { return sodecl_f64(::fabs(a.v)); }
-__device__ __forceinline__ sodecl_f64 ldexp(sodecl_f64 a, int k) { return sodecl_f64(::ldexp(a.v, k)); }
-__device__ __forceinline__ bool isnan(sodecl_f64 a) { return ::isnan(a.v); }
-__device__ __forceinline__ bool isinf(sodecl_f64 a) { return ::isinf(a.v); }
-__device__ __forceinline__ bool isfinite(sodecl_f64 a) { return ::isfinite(a.v); }
-__device__ __forceinline__ bool signbit(sodecl_f64 a) { return ::signbit(a.v); }
-__device__ __forceinline__ void sincos(sodecl_f64 a, sodecl_f64 *s, sodecl_f64 *c) { ::sincos(a.v, &s->v, &c->v); }
+__device__ __forceinline__ sodecl_num operator+(sodecl_num a) { return a; }
+__device__ __forceinline__ sodecl_num operator-(sodecl_num a) { return sodecl_num(-a.v); }
+__device__ __forceinline__ sodecl_num operator+(sodecl_num a, sodecl_num b) { return sodecl_num(a.v + b.v); }
+__device__ __forceinline__ sodecl_num operator-(sodecl_num a, sodecl_num b) { return sodecl_num(a.v - b.v); }
+__device__ __forceinline__ sodecl_num operator*(sodecl_num a, sodecl_num b) { return sodecl_num(a.v * b.v); }
+__device__ __forceinline__ sodecl_num operator/(sodecl_num a, sodecl_num b) { return sodecl_num(sodecl_div_rcp(a.v, b.v)); }
+__device__ __forceinline__ bool operator<(sodecl_num a, sodecl_num b) { return a.v < b.v; }
+__device__ __forceinline__ bool operator>(sodecl_num a, sodecl_num b) { return a.v > b.v; }
+__device__ __forceinline__ bool operator<=(sodecl_num a, sodecl_num b) { return a.v <= b.v; }
+__device__ __forceinline__ bool operator>=(sodecl_num a, sodecl_num b) { return a.v >= b.v; }
+__device__ __forceinline__ bool operator==(sodecl_num a, sodecl_num b) { return a.v == b.v; }
+__device__ __forceinline__ bool operator!=(sodecl_num a, sodecl_num b) { return a.v != b.v; }
+#define SODECL_NUM_UNARY(fn) \
+    __device__ __forceinline__ sodecl_num fn(sodecl_num a) { return sodecl_num(::fn(a.v)); }
+SODECL_NUM_UNARY(exp) SODECL_NUM_UNARY(exp2) SODECL_NUM_UNARY(expm1) SODECL_NUM_UNARY(log)
+SODECL_NUM_UNARY(log2) SODECL_NUM_UNARY(log10) SODECL_NUM_UNARY(log1p) SODECL_NUM_UNARY(sqrt)
+SODECL_NUM_UNARY(rsqrt) SODECL_NUM_UNARY(cbrt) SODECL_NUM_UNARY(sin) SODECL_NUM_UNARY(cos)
+SODECL_NUM_UNARY(tan) SODECL_NUM_UNARY(asin) SODECL_NUM_UNARY(acos) SODECL_NUM_UNARY(atan)
+SODECL_NUM_UNARY(sinh) SODECL_NUM_UNARY(cosh) SODECL_NUM_UNARY(tanh) SODECL_NUM_UNARY(asinh)
+SODECL_NUM_UNARY(acosh) SODECL_NUM_UNARY(atanh) SODECL_NUM_UNARY(fabs) SODECL_NUM_UNARY(floor)
+SODECL_NUM_UNARY(ceil) SODECL_NUM_UNARY(trunc) SODECL_NUM_UNARY(round) SODECL_NUM_UNARY(rint)
+SODECL_NUM_UNARY(erf) SODECL_NUM_UNARY(erfc) SODECL_NUM_UNARY(tgamma) SODECL_NUM_UNARY(lgamma)
+#define SODECL_NUM_BINARY(fn) \
+    __device__ __forceinline__ sodecl_num fn(sodecl_num a, sodecl_num b) { return sodecl_num(::fn(a.v, b.v)); }
+SODECL_NUM_BINARY(pow) SODECL_NUM_BINARY(fmin) SODECL_NUM_BINARY(fmax) SODECL_NUM_BINARY(fmod)
+SODECL_NUM_BINARY(atan2) SODECL_NUM_BINARY(hypot) SODECL_NUM_BINARY(copysign) SODECL_NUM_BINARY(fdim)
+SODECL_NUM_BINARY(remainder)
+__device__ __forceinline__ sodecl_num fma(sodecl_num a, sodecl_num b, sodecl_num c) { return sodecl_num(::fma(a.v, b.v, c.v)); }
+__device__ __forceinline__ sodecl_num abs(sodecl_num a) { return sodecl_num(::fabs(a.v)); }
+__device__ __forceinline__ sodecl_num ldexp(sodecl_num a, int k) { return sodecl_num(::ldexp(a.v, k)); }
+__device__ __forceinline__ bool isnan(sodecl_num a) { return ::isnan(a.v); }
+__device__ __forceinline__ bool isinf(sodecl_num a) { return ::isinf(a.v); }
+__device__ __forceinline__ bool isfinite(sodecl_num a) { return ::isfinite(a.v); }
+__device__ __forceinline__ bool signbit(sodecl_num a) { return ::signbit(a.v); }
+__device__ __forceinline__ void sincos(sodecl_num a, sodecl_num *s, sodecl_num *c) { ::sincos(a.v, &s->v, &c->v); }
 #endif
 
-#if SODECL_FP32
+#if SODECL_FAST_DIV
+typedef sodecl_num real_t;
+#elif SODECL_FP32
 typedef float real_t;
-#elif SODECL_FAST_DIV
-typedef sodecl_f64 real_t;
 #else
 typedef double real_t;
 #endif
@@ -133,12 +139,12 @@ __device__ __forceinline__ float sign(float x) { return x > 0.0f ? 1.0f : (x < 0
 __device__ __forceinline__ double sincos(double x, double *c) { double s; ::sincos(x, &s, c); return s; }
 __device__ __forceinline__ float sincos(float x, float *c) { float s; ::sincosf(x, &s, c); return s; }
 #if SODECL_FAST_DIV
-__device__ __forceinline__ sodecl_f64 sincos(sodecl_f64 x, sodecl_f64 *c) { double s; ::sincos(x.v, &s, &c->v); return sodecl_f64(s); }
-__device__ __forceinline__ sodecl_f64 mad(sodecl_f64 a, sodecl_f64 b, sodecl_f64 c) { return a * b + c; }
-__device__ __forceinline__ sodecl_f64 pown(sodecl_f64 x, int n) { return pow(x, sodecl_f64((double)n)); }
-__device__ __forceinline__ sodecl_f64 clamp(sodecl_f64 x, sodecl_f64 lo, sodecl_f64 hi) { return fmin(fmax(x, lo), hi); }
-__device__ __forceinline__ sodecl_f64 mix(sodecl_f64 a, sodecl_f64 b, sodecl_f64 t) { return a + (b - a) * t; }
-__device__ __forceinline__ sodecl_f64 sign(sodecl_f64 x) { return sodecl_f64(sign(x.v)); }
+__device__ __forceinline__ sodecl_num sincos(sodecl_num x, sodecl_num *c) { sodecl_num_t s; ::sincos(x.v, &s, &c->v); return sodecl_num(s); }
+__device__ __forceinline__ sodecl_num mad(sodecl_num a, sodecl_num b, sodecl_num c) { return a * b + c; }
+__device__ __forceinline__ sodecl_num pown(sodecl_num x, int n) { return pow(x, sodecl_num((sodecl_num_t)n)); }
+__device__ __forceinline__ sodecl_num clamp(sodecl_num x, sodecl_num lo, sodecl_num hi) { return fmin(fmax(x, lo), hi); }
+__device__ __forceinline__ sodecl_num mix(sodecl_num a, sodecl_num b, sodecl_num t) { return a + (b - a) * t; }
+__device__ __forceinline__ sodecl_num sign(sodecl_num x) { return sodecl_num(sign(x.v)); }
 #endif
 // native_/half_ variants: OpenCL allows them to be inaccurate; here they
 // are the accurate functions, so results do not depend on the spelling

@@ -15,7 +15,7 @@
 //   SODECL_SOLVER        0 Euler-Maruyama, 1 Euler, 2 RK4, 3 implicit Euler,
 //                        4 implicit midpoint (solver_Type numbering)
 //   SODECL_FP32          compute in float
-//   SODECL_FAST_DIV      FP64 through sodecl_f64 (exact reciprocal quotients)
+//   SODECL_FAST_DIV      arithmetic through sodecl_num (exact reciprocal quotients)
 //   SODECL_RECORD_F32    store records as float (else double)
 //   SODECL_HAS_JACOBIAN  the system file defines calc_jacobian
 //   SODECL_HAS_STOCH     the system file defines sode_system_stoch
@@ -47,15 +47,15 @@ typedef double sodecl_record_t;
 __device__ __forceinline__ double sodecl_qdiv(double a, double b) { return a / b; }
 __device__ __forceinline__ float sodecl_qdiv(float a, float b) { return a / b; }
 #if SODECL_FAST_DIV
-__device__ __forceinline__ sodecl_f64 sodecl_qdiv(sodecl_f64 a, sodecl_f64 b) { return sodecl_f64(a.v / b.v); }
+__device__ __forceinline__ sodecl_num sodecl_qdiv(sodecl_num a, sodecl_num b) { return sodecl_num(a.v / b.v); }
 #endif
 
 // A pivot that divides twice (the banded solve's forward multiplier and back
 // substitution): in reciprocal-division programs its reciprocal is taken once
 // and each quotient finished from it (sodecl_div_by, the IEEE quotient's bits).
 #if SODECL_FAST_DIV
-__device__ __forceinline__ real_t sodecl_pivot_rcp(real_t d) { return sodecl_f64(1.0 / d.v); }
-__device__ __forceinline__ real_t sodecl_pdiv(real_t a, real_t d, real_t r) { return sodecl_f64(sodecl_div_by(a.v, d.v, r.v)); }
+__device__ __forceinline__ real_t sodecl_pivot_rcp(real_t d) { return sodecl_num((sodecl_num_t)1 / d.v); }
+__device__ __forceinline__ real_t sodecl_pdiv(real_t a, real_t d, real_t r) { return sodecl_num(sodecl_div_by(a.v, d.v, r.v)); }
 #else
 __device__ __forceinline__ real_t sodecl_pivot_rcp(real_t d) { return d; }
 __device__ __forceinline__ real_t sodecl_pdiv(real_t a, real_t d, real_t) { return sodecl_qdiv(a, d); }
@@ -524,9 +524,9 @@ __device__ __forceinline__ sodecl_lanes_view sodecl_lanes_slot(real_t *slot, int
 __device__ __forceinline__ double sodecl_shfl(unsigned m, double x, int src) { return __shfl_sync(m, x, src, SODECL_LANES); }
 __device__ __forceinline__ float sodecl_shfl(unsigned m, float x, int src) { return __shfl_sync(m, x, src, SODECL_LANES); }
 #if SODECL_FAST_DIV
-__device__ __forceinline__ sodecl_f64 sodecl_shfl(unsigned m, sodecl_f64 x, int src)
+__device__ __forceinline__ sodecl_num sodecl_shfl(unsigned m, sodecl_num x, int src)
 {
-    return sodecl_f64(__shfl_sync(m, x.v, src, SODECL_LANES));
+    return sodecl_num(__shfl_sync(m, x.v, src, SODECL_LANES));
 }
 #endif
 

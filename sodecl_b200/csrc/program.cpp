@@ -425,8 +425,8 @@ std::string assemble(const ProgramSpec &spec, const std::string &system_src, con
         std::snprintf(buf, sizeof buf, "#define SODECL_RTOL %a\n#define SODECL_ATOL %a\n", spec.rtol, spec.atol);
         s << buf << "#define SODECL_MAX_STEPS " << spec.max_steps << "\n";
     }
-    if (spec.fp32) s << "#define double float\n";
-    else if (spec.fast_div) s << "#define double sodecl_f64\n";
+    if (spec.fast_div) s << "#define double sodecl_num\n";
+    else if (spec.fp32) s << "#define double float\n";
     s << "#line 1 \"system.cl\"\n";
     const std::string user = relax_parameter_bounds(system_src);
     s << (spec.fp32 ? suffix_float_literals(user) : user) << "\n";
@@ -565,7 +565,7 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
         s << "#define _epsilon1_ " << print_like_reference(sp.newton_tol) << "\n";
         s << l2_bound_define(sp.newton_tol, false);
         s << "namespace sodecl_cls_" << k << " {\n";
-        if (fast_div) s << "#define double sodecl_f64\n";
+        if (fast_div) s << "#define double sodecl_num\n";
         s << "#line 1 \"class" << k << ".cl\"\n" << relax_parameter_bounds(src) << "\n";
         if (fast_div) s << "#undef double\n";
         for (const auto &m : defined_macros(src)) s << "#undef " << m << "\n";
@@ -618,7 +618,7 @@ std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, in
     s << l2_bound_define(spec.newton_tol, false);
     const std::string user = relax_parameter_bounds(src);
     const std::vector<std::string> macros = defined_macros(src);
-    if (fast_div) s << "#define double sodecl_f64\n";
+    if (fast_div) s << "#define double sodecl_num\n";
     s << "#line 1 \"system.cl\"\n" << user << "\n";
     if (fast_div) s << "#undef double\n";
     for (const auto &m : macros) s << "#undef " << m << "\n";
@@ -668,7 +668,6 @@ std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string 
 {
     const SystemTraits traits = inspect_system(system_src);
     ProgramSpec s = spec;
-    if (s.fp32) s.fast_div = false;
     // the wrapper type would hand a struct to printf's varargs
     if (s.fast_div && system_src.find("printf") != std::string::npos) s.fast_div = false;
     if (!s.fast_div) return compile_one(s, system_src, traits);

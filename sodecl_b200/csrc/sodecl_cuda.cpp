@@ -408,6 +408,14 @@ int launch(sodecl_ctx *ctx, const DeviceArgs &a, cudaStream_t stream)
     return launch_kernel(ctx, ctx->kernel, ctx->cfg, a, stream);
 }
 
+// SODECL_DIV_DEFAULT: the reciprocal form in FP64 (faster on converging and
+// diverged orbits alike), IEEE division in FP32 (the reciprocal form gains
+// only on diverged orbits there; the tuner times both)
+bool reciprocal_division(const sodecl_cfg &c)
+{
+    return c.division == SODECL_DIV_RECIPROCAL || (c.division == SODECL_DIV_DEFAULT && c.precision == SODECL_FP64);
+}
+
 ProgramSpec make_spec(const sodecl_cfg &c)
 {
     ProgramSpec spec;
@@ -441,7 +449,7 @@ ProgramSpec make_spec(const sodecl_cfg &c)
     if (spec.min_blocks == 0 && lanes_of(c) == 1 && c.solver == SODECL_RUNGE_KUTTA && !spec.fp32 &&
         c.num_equat <= 8)
         spec.min_blocks = std::max(1, 65536 / (spec.block_max * 85));
-    spec.fast_div = c.division == SODECL_DIV_RECIPROCAL;
+    spec.fast_div = reciprocal_division(c);
     spec.lanes = lanes_of(c);
     spec.rtol = c.rtol;
     spec.atol = c.atol;
@@ -463,7 +471,7 @@ void sodecl_cfg_init(sodecl_cfg *cfg)
     cfg->fmad = 1;
     cfg->newton_tol = 1e-7;
     cfg->newton_max_iter = 1000;
-    cfg->division = SODECL_DIV_RECIPROCAL;
+    cfg->division = SODECL_DIV_DEFAULT;
     cfg->rtol = 1e-6;
     cfg->atol = 1e-9;
     cfg->max_steps = 100000;
@@ -520,7 +528,8 @@ int sodecl_cuda_create(const sodecl_cfg *cfg, sodecl_ctx **out)
     if (c.local_group_size < 0 || c.local_group_size > 1024) return SODECL_ERR_INVALID_ARG;
     if (c.newton_tol < 0 || !std::isfinite(c.newton_tol) || c.newton_max_iter < 0) return SODECL_ERR_INVALID_ARG;
     if (c.min_blocks_per_sm < 0 || c.min_blocks_per_sm > 32) return SODECL_ERR_INVALID_ARG;
-    if (c.division != SODECL_DIV_RECIPROCAL && c.division != SODECL_DIV_IEEE) return SODECL_ERR_INVALID_ARG;
+    if (c.division != SODECL_DIV_RECIPROCAL && c.division != SODECL_DIV_IEEE && c.division != SODECL_DIV_DEFAULT)
+        return SODECL_ERR_INVALID_ARG;
     if (c.lanes_per_orbit < 0 || c.lanes_per_orbit > 32 || (c.lanes_per_orbit & (c.lanes_per_orbit - 1)) != 0)
         return SODECL_ERR_INVALID_ARG;
     const int64_t nchunks = count_chunks(c);
@@ -896,11 +905,9 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
     };
     std::vector<Cand> cands = {{128, 0, SODECL_DIV_IEEE, 1}, {128, 4, SODECL_DIV_IEEE, 1},
                                {256, 3, SODECL_DIV_IEEE, 1}, {64, 0, SODECL_DIV_IEEE, 1}};
-    if (ctx->cfg.precision == SODECL_FP64) {
-        cands.push_back({128, 0, SODECL_DIV_RECIPROCAL, 1});
-        cands.push_back({128, 4, SODECL_DIV_RECIPROCAL, 1});
-        cands.push_back({128, 3, SODECL_DIV_RECIPROCAL, 1});
-    }
+    cands.push_back({128, 0, SODECL_DIV_RECIPROCAL, 1});
+    cands.push_back({128, 4, SODECL_DIV_RECIPROCAL, 1});
+    if (ctx->cfg.precision == SODECL_FP64) cands.push_back({128, 3, SODECL_DIV_RECIPROCAL, 1});
     // lanes per orbit: up to the first power of two >= the equations
     const auto traits = sodecl_b200::inspect_system(ctx->system_src);
     const int solver = ctx->cfg.solver;
@@ -1062,7 +1069,7 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     // passes with gradients use IEEE division, measured faster there (the
     // reciprocal wrapper costs registers the backward sweep needs).  The
     // quotients are the same either way.
-    const bool fast_div = !with_gradient && ctx->cfg.division == SODECL_DIV_RECIPROCAL;
+    const bool fast_div = !with_gradient && reciprocal_division(ctx->cfg);
     if (!ctx->adj_prog || ctx->adj_tape != tape || ctx->adj_mode != mode || ctx->adj_min_blocks != min_blocks ||
         ctx->adj_fast_div != fast_div || ctx->adj_block != block) {
         try {

@@ -138,11 +138,12 @@ def test_midpoint_stop_bound_is_exact(precision, tol):
         v = np.nextafter(v, ft(np.inf))
 
 
-def test_fp32_program_rewrites_literals():
-    rc, ctx = _create(precision=1)
+@pytest.mark.parametrize("division,scalar", [(N.DIV_IEEE, "float"), (N.DIV_RECIPROCAL, "sodecl_num")])
+def test_fp32_program_rewrites_literals(division, scalar):
+    rc, ctx = _create(precision=1, division=division)
     assert _compile(ctx, open(system_path("oculomotor")).read()) == N.OK
     text = N.program_source(ctx)
-    assert "#define double float" in text
+    assert "#define double %s" % scalar in text
     assert "#define OCM_T1 0.15f" in text and "(1.00f / p[2])" in text
     assert "/* burst-neuron firing-rate non-linearity:" in text  # comments untouched
     N.lib.sodecl_cuda_destroy(ctx)
@@ -234,19 +235,27 @@ def test_python_module_fails_cleanly_without_device():
 
 
 def test_division_modes_and_fallback():
-    """FP64 programs build with the reciprocal quotient; a system file that
-    needs plain double (an implicit conversion) falls back to IEEE division."""
+    """The default: the reciprocal quotient in FP64, IEEE division in FP32;
+    either precision builds the reciprocal form when asked.  A system file
+    that needs the plain scalar (an implicit conversion) falls back to IEEE
+    division."""
     kw = dict(dt=1e-3, tspan=0.1, ksteps=10, neq=6, npar=6, orbits=4)
     assert Integrator(system_path("oculomotor"), "rk4", division="reciprocal", **kw).division == "reciprocal"
     assert Integrator(system_path("oculomotor"), "rk4", **kw).division == "reciprocal"  # the default
     assert Integrator(system_path("oculomotor"), "rk4", division="ieee", **kw).division == "ieee"
-    assert Integrator(system_path("oculomotor"), "rk4", division="reciprocal", precision="fp32", **kw).division == "ieee"
+    assert Integrator(system_path("oculomotor"), "rk4", precision="fp32", **kw).division == "ieee"  # the default
+    assert Integrator(system_path("oculomotor"), "rk4", division="reciprocal", precision="fp32",
+                      **kw).division == "reciprocal"
+    assert Integrator(system_path("oculomotor"), "rk4", division="ieee", precision="fp32", **kw).division == "ieee"
     src = open(system_path("oculomotor")).read().replace("double drive = y[3] - y[4];", "float drive = y[3] - y[4];")
-    sim = Integrator(None, "rk4", system_src=src, division="reciprocal", **kw)
-    assert sim.division == "ieee"
-    assert "#define SODECL_FAST_DIV 0" in sim.program_source
+    for prec in ("fp64", "fp32"):
+        sim = Integrator(None, "rk4", system_src=src, division="reciprocal", precision=prec, **kw)
+        assert sim.division == "ieee"
+        assert "#define SODECL_FAST_DIV 0" in sim.program_source
     text = Integrator(system_path("oculomotor"), "rk4", division="reciprocal", **kw).program_source
-    assert "#define SODECL_FAST_DIV 1" in text and "#define double sodecl_f64" in text
+    assert "#define SODECL_FAST_DIV 1" in text and "#define double sodecl_num" in text
+    with pytest.raises(ValueError):
+        Integrator(system_path("oculomotor"), "rk4", division="fast", **kw)
 
 
 def test_get_cfg_returns_the_configuration():

@@ -409,6 +409,40 @@ def test_reciprocal_quotient_equals_ieee_division():
     assert bad.value == 0, "first differing pair %r / %r" % (a.value, b.value)
 
 
+def test_reciprocal_quotient_f32_equals_ieee_division():
+    bad, a, b = C.c_int64(), C.c_float(), C.c_float()
+    N.check(N.lib.sodecl_cuda_division_check_f32(0, 1 << 33, 20240602, C.byref(bad), C.byref(a), C.byref(b)))
+    assert bad.value == 0, "first differing pair %r / %r" % (a.value, b.value)
+
+
+@pytest.mark.parametrize("system,solver,dt", [("oculomotor", "rk4", 1e-3), ("oculomotor", "rk4", 1e-5),
+                                              ("oculomotor", "im", 1e-3), ("kuramoto", "se", 0.01)])
+def test_fp32_division_modes_give_identical_records(system, solver, dt):
+    """FP32 programs: the reciprocal quotient and IEEE division (the default)
+    give the same records, diverging orbits (dt 1e-3) included."""
+    n = 2048
+    if system == "oculomotor":
+        t0, y0, p = oculomotor_inputs(n, 17)
+        kw = dict(neq=6, npar=6)
+        cnt = None
+    else:
+        rng = np.random.default_rng(18)
+        N_osc = 16
+        p = np.concatenate([rng.uniform(0, 5, (n, 1)), np.tile(rng.normal(size=N_osc), (n, 1)),
+                            rng.uniform(0, 0.5, (n, N_osc))], axis=1)
+        t0, y0, cnt = np.zeros(n), rng.uniform(0, 2 * np.pi, (n, N_osc)), np.arange(n) * 4096.0
+        kw = dict(neq=N_osc, npar=2 * N_osc + 1, nnoi=N_osc)
+    kw.update(dt=dt, tspan=400 * dt, ksteps=40, precision="fp32", newton_tol=1e-4)
+    out = {}
+    for mode in ("default", "ieee", "reciprocal"):
+        with Integrator(system_path(system), solver, orbits=n, division=mode, **kw) as sim:
+            assert sim.division == ("ieee" if mode == "default" else mode)
+            sim.upload(t0, y0, p, cnt)
+            out[mode] = sim.run()
+    np.testing.assert_array_equal(out["reciprocal"], out["ieee"])
+    np.testing.assert_array_equal(out["default"], out["ieee"])
+
+
 @pytest.mark.parametrize("fmad", [0, 1])
 @pytest.mark.parametrize("system,solver,dt", [("oculomotor", "rk4", 1e-5), ("oculomotor", "ie", 1e-3),
                                               ("oculomotor", "im", 1e-3), ("oculomotor", "euler", 1e-6),
