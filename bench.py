@@ -451,11 +451,17 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
     sim = Integrator(system_path("oculomotor"), "rk4", orbits=n, **kw)
     assert sim.num_chunks * ksteps == nsteps
     T = lambda x: torch.tensor(x, device=dev)  # noqa: E731
+    # the library's default schedule: the forward sweep records the whole
+    # trajectory (n x nsteps x 25 doubles, 65.5 GB here) when it fits in half
+    # the free memory; the same context then serves the other schedules
     adj = Adjoint(sim)
-    adj_tape = Adjoint(sim, use_tape=True)
+    sqrt_every = int(np.ceil(np.sqrt(nsteps)))
+    adj_sqrt = Adjoint(sim, ckpt_every=sqrt_every)
+    adj_tape = Adjoint(sim, use_tape=True, ckpt_every=nsteps)
     # the same file without calc_vjp: products from calc_jacobian + calc_jacobian_params
     src = open(system_path("oculomotor")).read().replace("void calc_vjp(", "void unused_calc_vjp(")
-    adj_jac = Adjoint(Integrator(None, "rk4", orbits=n, system_src=src, **kw))
+    sim_jac = Integrator(None, "rk4", orbits=n, system_src=src, **kw)
+    adj_jac = Adjoint(sim_jac, ckpt_every=nsteps)
     wide = Adjoint(Integrator(system_path("oculomotor"), "rk4", orbits=n * 24, **kw))
     t0, y0d, gd = T(np.zeros(n)), T(y0), T(guess)
 
@@ -472,8 +478,13 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
             out.append(s.elapsed_time(e))
         return float(np.median(out)), r
 
+    whole_gb = 8.0 * n * (nsteps * 25 + 7) / 1e9
+    whole = whole_gb * 1e9 <= 0.5 * torch.cuda.mem_get_info(dev)[0]  # the library's test, before its first call
     ms_adj, (loss, gp, gy, flags) = timed(lambda: adj(t0, y0d, gd, targets))
+    ms_sqrt, (loss_s, gp_s, gy_s, _) = timed(lambda: adj_sqrt(t0, y0d, gd, targets))
+    sqrt_identical = bool(torch.equal(loss_s, loss) and torch.equal(gp_s, gp) and torch.equal(gy_s, gy))
     ms_jac, (_, gpj, _, _) = timed(lambda: adj_jac(t0, y0d, gd, targets))
+    sim_jac.close()
     ms_tape, (_, gpt, gyt, _) = timed(lambda: adj_tape(t0, y0d, gd, targets), reps=1)
     ms_fd, (fp, fy) = timed(lambda: finite_difference_gradient(t0, y0d, gd, targets, wide))
     ms_fwd, _ = timed(lambda: adj(t0, y0d, gd, targets, with_gradient=False))
@@ -491,6 +502,10 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
             "adjoint_jacobians_ms": ms_jac, "adjoint_tape_ms": ms_tape,
             "rel_diff_jacobians_vs_vjp": err_jac, "rel_diff_tape_vs_vjp": err_tape,
             "finite_difference_ms": ms_fd, "loss_only_ms": ms_fwd, "speedup_vs_fd": ms_fd / ms_adj,
+            "schedule": ("forward sweep records the whole trajectory (%.1f GB), no recomputation" % whole_gb
+                         if whole else "checkpoints every %d steps (the whole trajectory did not fit)" % sqrt_every),
+            "adjoint_sqrt_checkpoints_ms": ms_sqrt, "sqrt_checkpoint_every": sqrt_every,
+            "speedup_vs_fd_sqrt_checkpoints": ms_fd / ms_sqrt, "sqrt_checkpoints_identical": sqrt_identical,
             "rel_diff_vs_fd_params": q(dp), "rel_diff_vs_fd_y0": q(dy),
             "tape_overflow": int((flags != 0).sum().item()),
             "fd": "central, relative step 1e-6, 24 perturbed copies per orbit in one launch",

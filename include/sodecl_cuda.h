@@ -121,11 +121,20 @@ typedef struct sodecl_cfg {
     double rtol;             /* SODECL_DORMAND_PRINCE: relative and absolute error per step, */
     double atol;             /*   err_i / (atol + rtol max(|y_i|, |y5_i|)) in RMS <= 1; default 1e-6, 1e-9 */
     int32_t max_steps;       /* SODECL_DORMAND_PRINCE: step attempts per record interval; default 100000 */
+    int32_t record_store;    /* how one thread per orbit writes its records: SODECL_STORE_DIRECT
+                                (default; one 8-byte store per equation, coalesced across the
+                                warp) or SODECL_STORE_PAIRS (neighbouring orbits swap values
+                                with a shuffle and each writes one equation of both as a
+                                16-byte store).  Same records either way; the tuner times both.
+                                No counterpart in the reference. */
 } sodecl_cfg;
 
+#define SODECL_STORE_DIRECT 0
+#define SODECL_STORE_PAIRS 1
+
 /* Fills the defaults: Euler, fp64, fmad on, Newton 1e-7 / 1000, device 0,
- * reciprocal division, one thread per orbit, rtol 1e-6, atol 1e-9, 100000
- * adaptive steps per record interval. */
+ * SODECL_DIV_DEFAULT division, one thread per orbit, direct record stores,
+ * rtol 1e-6, atol 1e-9, 100000 adaptive steps per record interval. */
 void sodecl_cfg_init(sodecl_cfg *cfg);
 
 /* Validates cfg and makes a context bound to cfg->device.  Needs no GPU
@@ -235,7 +244,13 @@ int sodecl_cuda_launch(sodecl_ctx *ctx, const sodecl_launch *launch, void *strea
  * calc_jacobian + calc_jacobian_params, else the right-hand side
  * differentiated in reverse mode (the system file compiled a second time
  * with a recording `double`).  The state is checkpointed every `ckpt_every`
- * steps (0: ~sqrt(steps)) and recomputed per segment.
+ * steps and recomputed per segment; with ckpt_every >= steps the forward
+ * sweep records the whole trajectory (steps x (4 num_equat + 1) doubles per
+ * orbit for RK4, num_equat + 1 otherwise) and nothing is recomputed.  The
+ * default picks that when the buffer takes at most half the free device
+ * memory, else ~sqrt(steps).  The context keeps the buffer for its next call
+ * (sodecl_cuda_destroy frees it).  Gradients are the same bit for bit with
+ * any spacing.
  * Records, steps and the step size follow the context's configuration; all
  * pointers are device pointers; the launch goes on `stream`.  No
  * counterpart in the reference. */
@@ -250,7 +265,8 @@ typedef struct sodecl_adjoint_io {
     int32_t *flags;         /* [n] out, or NULL: 4 = tape overflow (raise tape_entries),
                                1 = a Newton step stopped at newton_max_iter */
     int64_t n;              /* orbits, <= list_size */
-    int32_t ckpt_every;     /* steps per checkpoint; 0 = ceil(sqrt(steps)) */
+    int32_t ckpt_every;     /* steps per checkpoint; 0 = the whole trajectory when it fits in half the
+                               free device memory, else ceil(sqrt(steps)) */
     int32_t tape_entries;   /* operations one right-hand side may record; 0 = 256 */
     int32_t use_tape;       /* 1: differentiate sode_system on the tape even when the system file
                                provides the products itself -- calc_vjp(t, y, v, ybar, pbar, p)
@@ -270,10 +286,12 @@ int sodecl_cuda_kernel_info(sodecl_ctx *ctx, int *regs, int *local_bytes, int *m
 /* Autotuner: times candidate launch shapes (threads per block, resident-block
  * hints, and lanes per orbit when the system file has sode_system_row and the
  * solver is explicit or stochastic) and division modes on copies of the
- * first `sample_orbits` uploaded orbits for `sample_steps` steps -- the
- * context's state does not advance -- and rebuilds the program with the
- * fastest.  All candidates give identical results.  Writes the choice (any
- * pointer may be NULL). */
+ * first `sample_orbits` uploaded orbits for `sample_steps` steps, records
+ * included -- the context's state does not advance -- then the winner with
+ * paired record stores (SODECL_STORE_PAIRS), and rebuilds the program with
+ * the fastest.  All candidates give identical results.  Writes the choice (any
+ * pointer may be NULL; the store form is in the configuration,
+ * sodecl_cuda_get_cfg). */
 int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_steps, int32_t *block,
                          int32_t *min_blocks, int32_t *division, int32_t *lanes, double *best_ms);
 

@@ -27,6 +27,7 @@ ABI_VERSION = 3
 STOCHASTIC_EULER, EULER, RUNGE_KUTTA, IMPLICIT_EULER, IMPLICIT_MIDPOINT, DORMAND_PRINCE = range(6)
 FP64, FP32 = 0, 1
 DIV_RECIPROCAL, DIV_IEEE, DIV_DEFAULT = 0, 1, 2
+STORE_DIRECT, STORE_PAIRS = 0, 1
 FLAG_NEWTON_CAP = 1
 FLAG_NONFINITE = 2
 
@@ -54,6 +55,7 @@ class Cfg(C.Structure):
         ("rtol", C.c_double),
         ("atol", C.c_double),
         ("max_steps", C.c_int32),
+        ("record_store", C.c_int32),
     ]
 
 

@@ -51,7 +51,7 @@ class Integrator:
     def __init__(self, system, solver, *, dt, tspan, ksteps, neq, npar, orbits, nnoi=0, device=0,
                  precision="fp64", fmad=True, newton_tol=1e-7, newton_max_iter=1000, block=0,
                  record_f32=False, min_blocks=0, division="default", lanes=1, system_src=None, rtol=1e-6,
-                 atol=1e-9, max_steps=100000):
+                 atol=1e-9, max_steps=100000, record_store="direct"):
         cfg = N.Cfg()
         N.lib.sodecl_cfg_init(C.byref(cfg))
         cfg.solver = _solver_id(solver)
@@ -78,6 +78,10 @@ class Integrator:
         cfg.rtol = float(rtol)
         cfg.atol = float(atol)
         cfg.max_steps = int(max_steps)
+        stores = {"direct": N.STORE_DIRECT, "pairs": N.STORE_PAIRS}
+        if str(record_store).lower() not in stores:
+            raise ValueError("record_store must be 'direct' or 'pairs', not %r" % (record_store,))
+        cfg.record_store = stores[str(record_store).lower()]
         self.cfg = cfg
         self._ctx = C.c_void_p()
         rc = N.lib.sodecl_cuda_create(C.byref(cfg), C.byref(self._ctx))
@@ -126,15 +130,17 @@ class Integrator:
         return "ieee" if N.lib.sodecl_cuda_program_division(self._ctx) == N.DIV_IEEE else "reciprocal"
 
     def autotune(self, sample_orbits=1 << 17, sample_steps=200):
-        """Picks threads per block, the resident-block hint, the division mode
-        and (for system files with sode_system_row) lanes per orbit by timing
-        them on copies of uploaded orbits; returns the choice."""
+        """Picks threads per block, the resident-block hint, the division mode,
+        (for system files with sode_system_row) lanes per orbit and the record
+        store form by timing them on copies of uploaded orbits; returns the
+        choice."""
         b, m, d, ln, ms = C.c_int32(), C.c_int32(), C.c_int32(), C.c_int32(), C.c_double()
         N.check(N.lib.sodecl_cuda_autotune(self._ctx, int(sample_orbits), int(sample_steps), C.byref(b), C.byref(m),
                                            C.byref(d), C.byref(ln), C.byref(ms)), self._ctx)
         N.check(N.lib.sodecl_cuda_get_cfg(self._ctx, C.byref(self.cfg)), self._ctx)
         return {"block": b.value, "min_blocks": m.value,
                 "division": "reciprocal" if d.value == N.DIV_RECIPROCAL else "ieee", "lanes": ln.value,
+                "record_store": "pairs" if self.cfg.record_store == N.STORE_PAIRS else "direct",
                 "sample_ms": ms.value}
 
     def kernel_info(self):

@@ -14,7 +14,9 @@
 // the state is checkpointed every `ckpt_every` steps: the backward pass
 // recomputes each segment's states from its checkpoint, then walks the
 // segment's steps in reverse.  Memory per orbit: T/C checkpoints and C
-// segment states (C ~ sqrt(T) balances the two).
+// segment states (C ~ sqrt(T) balances the two).  With C >= T there is one
+// segment, which the forward sweep records as it goes: T segment states and
+// no recomputation.
 //
 // Part 1 (before the user file): the tape and the sodecl_ad type.
 // Part 2 (SODECL_ADJOINT_KERNEL, after both copies of the user file): the
@@ -411,6 +413,37 @@ __device__ __forceinline__ void sodecl_step_adjoint(double h, double t, const do
 #define SODECL_SEG_WIDTH (_numeq_ + 1)
 #endif
 
+// One step of the forward arithmetic (sodecl_advance's), recording into st
+// (stride n between values) unless it is null: the state and t before the
+// step and, for RK4, its three stage inputs.  The forward sweep and the
+// segment recomputation both step through here, so they agree bit for bit.
+__device__ __forceinline__ void sodecl_adjoint_step(real_t &t, real_t *y, real_t *p, long long i, double &counter,
+                                                    sodecl_i64 &passes, int &capped, double *st, long long n)
+{
+    if (st) {
+        st[_numeq_ * n] = (double)t;
+        for (int e = 0; e < _numeq_; ++e) st[e * n] = (double)y[e];
+    }
+#if SODECL_SOLVER == 2
+    (void)i;
+    (void)counter;
+    (void)passes;
+    (void)capped;
+    real_t x2[_numeq_], x3[_numeq_], x4[_numeq_], ynew[_numeq_];
+    sodecl_step_rk4(_m_dt_, t, y, ynew, p, x2, x3, x4);
+    t = t + _m_dt_;
+    for (int e = 0; e < _numeq_; ++e) y[e] = ynew[e];
+    if (st)
+        for (int e = 0; e < _numeq_; ++e) {
+            st[(_numeq_ + 1 + e) * n] = (double)x2[e];
+            st[(2 * _numeq_ + 1 + e) * n] = (double)x3[e];
+            st[(3 * _numeq_ + 1 + e) * n] = (double)x4[e];
+        }
+#else
+    sodecl_advance(t, y, p, i, counter, passes, capped);
+#endif
+}
+
 struct sodecl_adjoint_args {
     const double *t0;         // [n]
     const double *y0;         // [n][neq]
@@ -421,7 +454,7 @@ struct sodecl_adjoint_args {
     double *grad_y0;          // [n][neq] or null
     double *ckpt;             // scratch [nckpt][neq][n]
     double *ckpt_t;           // scratch [nckpt][n]
-    double *seg;              // scratch [ckpt_every][SODECL_SEG_WIDTH][n]: state, t, (RK4) stage inputs
+    double *seg;              // scratch [min(ckpt_every, steps)][SODECL_SEG_WIDTH][n]: state, t, (RK4) stage inputs
     int *flags;               // [n] or null
     long long n;
     int nchunks;              // records - 1; steps = nchunks * _numsteps_
@@ -446,7 +479,10 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
     sodecl_i64 passes = 0;
     int capped = 0;
 
-    // forward: loss at every record, checkpoints every C steps
+    // forward: loss at every record, checkpoints every C steps; with one
+    // segment (C >= steps) the sweep records the segment itself, and the
+    // backward pass has nothing to recompute
+    const bool whole = a.grad_p && C >= steps;
     double loss = 0.0;
     for (int s = 0; s <= steps; ++s) {
         if (s % _numsteps_ == 0) {
@@ -456,12 +492,14 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
                 loss += d * d;
             }
         }
-        if (a.grad_p && s % C == 0 && s < steps) {
+        if (a.grad_p && !whole && s % C == 0 && s < steps) {
             const long long c = s / C;
             a.ckpt_t[c * n + i] = (double)t;
             for (int e = 0; e < _numeq_; ++e) a.ckpt[(c * _numeq_ + e) * n + i] = (double)y[e];
         }
-        if (s < steps) sodecl_advance(t, y, p, i, counter, passes, capped);
+        if (s < steps)
+            sodecl_adjoint_step(t, y, p, i, counter, passes, capped,
+                                whole ? a.seg + (long long)s * SODECL_SEG_WIDTH * n + i : nullptr, n);
     }
     a.loss[i] = loss * w;
     if (!a.grad_p) {
@@ -488,27 +526,13 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
     for (int sg = nseg - 1; sg >= 0; --sg) {
         const int s0 = sg * C, s1 = min(steps, s0 + C);
         // recompute the segment's states from its checkpoint
-        real_t ys[_numeq_];
-        real_t ts = (real_t)a.ckpt_t[(long long)sg * n + i];
-        for (int e = 0; e < _numeq_; ++e) ys[e] = (real_t)a.ckpt[((long long)sg * _numeq_ + e) * n + i];
-        for (int s = s0; s < s1; ++s) {
-            double *st = a.seg + (long long)(s - s0) * SODECL_SEG_WIDTH * n + i;
-            st[_numeq_ * n] = (double)ts;
-            for (int e = 0; e < _numeq_; ++e) st[e * n] = (double)ys[e];
-#if SODECL_SOLVER == 2
-            // the step with its stage inputs recorded (sodecl_advance's RK4 step)
-            real_t x2[_numeq_], x3[_numeq_], x4[_numeq_], ynew[_numeq_];
-            sodecl_step_rk4(_m_dt_, ts, ys, ynew, p, x2, x3, x4);
-            ts = ts + _m_dt_;
-            for (int e = 0; e < _numeq_; ++e) {
-                ys[e] = ynew[e];
-                st[(_numeq_ + 1 + e) * n] = (double)x2[e];
-                st[(2 * _numeq_ + 1 + e) * n] = (double)x3[e];
-                st[(3 * _numeq_ + 1 + e) * n] = (double)x4[e];
-            }
-#else
-            sodecl_advance(ts, ys, p, i, counter, passes, capped);
-#endif
+        if (!whole) {
+            real_t ys[_numeq_];
+            real_t ts = (real_t)a.ckpt_t[(long long)sg * n + i];
+            for (int e = 0; e < _numeq_; ++e) ys[e] = (real_t)a.ckpt[((long long)sg * _numeq_ + e) * n + i];
+            for (int s = s0; s < s1; ++s)
+                sodecl_adjoint_step(ts, ys, p, i, counter, passes, capped,
+                                    a.seg + (long long)(s - s0) * SODECL_SEG_WIDTH * n + i, n);
         }
         // reverse the segment's steps
         for (int s = s1 - 1; s >= s0; --s) {

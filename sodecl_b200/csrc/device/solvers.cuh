@@ -28,10 +28,18 @@
 //                        file defines sode_system_row / sode_system_stoch_row /
 //                        calc_jacobian_band
 //   SODECL_HAS_ROW_BAND  the system file defines sode_system_row_band
+//   SODECL_PAIR_STORES   one-thread kernel: records written two orbits per
+//                        vector store (sodecl_store_pairs)
 
 #ifndef SODECL_MIN_BLOCKS
 #define SODECL_MIN_BLOCKS 1
 #endif
+#ifndef SODECL_PAIR_STORES
+#define SODECL_PAIR_STORES 0
+#endif
+template <class T> struct sodecl_pair_of;
+template <> struct sodecl_pair_of<double> { typedef double2 type; };
+template <> struct sodecl_pair_of<float> { typedef float2 type; };
 #ifndef SODECL_LANES
 #define SODECL_LANES 1
 #endif
@@ -796,16 +804,51 @@ __device__ __forceinline__ void sodecl_lanes_advance(real_t &t, real_t *yown, co
 #endif  // SODECL_LANES > 1
 
 #ifndef SODECL_STEPS_ONLY
+#if SODECL_PAIR_STORES
+// Paired stores: the two threads of orbits 2k and 2k+1 (lanes 2j, 2j+1) swap
+// one value per two equations with a shuffle, so that the even thread writes
+// equation e of both orbits and the odd thread equation e+1 of both, each as
+// one vector store (16 bytes for double records): half the store
+// instructions, the same bytes and sectors.  Needs an even block size, an
+// even first column and row stride and a base aligned to a pair, all uniform
+// across the launch; an orbit whose partner is past the end stores alone.
+__device__ __forceinline__ bool sodecl_store_pairs(const sodecl_args &a, sodecl_record_t *row, sodecl_i64 i,
+                                                   const real_t *y)
+{
+    typedef typename sodecl_pair_of<sodecl_record_t>::type pair_t;
+    const bool layout = (blockDim.x % 2u) == 0u && (a.rec_col0 % 2) == 0 && (a.rec_stride % 2) == 0 &&
+                        ((unsigned long long)a.records % sizeof(pair_t)) == 0ull;
+    const int odd = (int)(i & 1);
+    if (!layout || (!odd && i + 1 >= a.n)) return false;
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned pair_mask = 3u << (lane & 30u);
+    sodecl_record_t *base = row - odd;  // column of the pair's even orbit
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e + 1 < _numeq_; e += 2) {
+        const sodecl_record_t v0 = (sodecl_record_t)y[e], v1 = (sodecl_record_t)y[e + 1];
+        const sodecl_record_t got = __shfl_xor_sync(pair_mask, odd ? v0 : v1, 1);
+        pair_t w;
+        w.x = odd ? got : v0;
+        w.y = odd ? v1 : got;
+        __stcs(reinterpret_cast<pair_t *>(base + (sodecl_i64)(e + odd) * a.rec_stride), w);
+    }
+    if (_numeq_ % 2) __stcs(row + (sodecl_i64)(_numeq_ - 1) * a.rec_stride, (sodecl_record_t)y[_numeq_ - 1]);
+    return true;
+}
+#endif
+
 __device__ __forceinline__ void sodecl_store_record(const sodecl_args &a, int rec, sodecl_i64 i, const real_t *y, int &flags)
 {
     sodecl_record_t *row = a.records + (sodecl_i64)(rec - a.rec_first) * _numeq_ * a.rec_stride + a.rec_col0 + i;
     bool finite = true;
 #pragma unroll SODECL_EQ_UNROLL
-    for (int e = 0; e < _numeq_; ++e) {
-        finite = finite && isfinite(y[e]);
-        __stcs(row + (sodecl_i64)e * a.rec_stride, (sodecl_record_t)y[e]);
-    }
+    for (int e = 0; e < _numeq_; ++e) finite = finite && isfinite(y[e]);
     if (!finite) flags |= SODECL_FLAG_NONFINITE;
+#if SODECL_PAIR_STORES
+    if (sodecl_store_pairs(a, row, i, y)) return;
+#endif
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) __stcs(row + (sodecl_i64)e * a.rec_stride, (sodecl_record_t)y[e]);
 }
 
 // The end of an orbit's launch: the closing record (on request), the state,

@@ -400,6 +400,7 @@ std::string assemble(const ProgramSpec &spec, const std::string &system_src, con
     s << "#define SODECL_BLOCK_MAX " << spec.block_max << "\n";
     if (spec.min_blocks > 0) s << "#define SODECL_MIN_BLOCKS " << spec.min_blocks << "\n";
     s << "#define SODECL_LANES " << spec.lanes << "\n";
+    if (spec.pair_stores) s << "#define SODECL_PAIR_STORES 1\n";
     s << "#define SODECL_HAS_ROW " << (traits.has_row ? 1 : 0) << "\n";
     s << "#define SODECL_HAS_STOCH_ROW " << (traits.has_stoch_row ? 1 : 0) << "\n";
     s << "#define SODECL_HAS_JAC_BAND " << (traits.has_jac_band ? 1 : 0) << "\n";

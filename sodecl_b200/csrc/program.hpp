@@ -25,6 +25,7 @@ struct ProgramSpec {
     int block_max = 256;
     int min_blocks = 0;
     int lanes = 1;           // lanes per orbit (1, or a power of two up to 32)
+    bool pair_stores = false;  // one thread per orbit: records two orbits per vector store
     double rtol = 1e-6;      // adaptive solver (solver 5): error tolerances and
     double atol = 1e-9;      // step attempts per record interval
     int max_steps = 100000;

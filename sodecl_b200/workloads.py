@@ -131,7 +131,7 @@ def _adjoint_main(a):
     sim = Integrator(system_path("oculomotor"), "rk4", dt=dt, tspan=(a.nsteps - 0.5) * dt, ksteps=a.ksteps, neq=6,
                      npar=6, orbits=a.orbits)
     T = lambda x: torch.tensor(x, device="cuda")  # noqa: E731
-    adj = Adjoint(sim)
+    adj = Adjoint(sim, ckpt_every=a.ckpt_every)
     for k in range(a.launches):
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
@@ -139,7 +139,7 @@ def _adjoint_main(a):
         e.record()
         torch.cuda.synchronize()
         print(json.dumps({"case": a.case, "launch": k, "ms": s.elapsed_time(e), "orbits": a.orbits,
-                          "nsteps": a.nsteps}), flush=True)
+                          "nsteps": a.nsteps, "ckpt_every": a.ckpt_every}), flush=True)
 
 
 def _parse():
@@ -154,8 +154,12 @@ def _parse():
     ap.add_argument("--lanes", type=int, default=1)
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--precision", default="fp64")
-    ap.add_argument("--division", default="ieee", choices=["ieee", "reciprocal"])
+    ap.add_argument("--division", default="ieee", choices=["default", "ieee", "reciprocal"])
+    ap.add_argument("--ckpt-every", type=int, default=0,
+                    help="adjoint-oculomotor: steps per checkpoint (0: the library's choice; >= nsteps: the "
+                         "forward sweep records the whole trajectory)")
     ap.add_argument("--min-blocks", type=int, default=0)
+    ap.add_argument("--record-store", default="direct", choices=["direct", "pairs"])
     ap.add_argument("--launches", type=int, default=2)
     ap.add_argument("--max-steps", type=int, default=10000, help="uneven-batch: longest step count")
     ap.add_argument("--system-file", default=None,
@@ -192,7 +196,7 @@ def main():
         raise SystemExit("unknown case " + a.case)
     sim = Integrator(a.system_file or system_path(system), solver, dt=dt, tspan=a.nsteps * dt, ksteps=a.ksteps, neq=neq,
                      npar=p.shape[1], nnoi=nnoi, orbits=n, precision=a.precision, lanes=a.lanes, block=a.block,
-                     division=a.division, min_blocks=a.min_blocks)
+                     division=a.division, min_blocks=a.min_blocks, record_store=a.record_store)
     dev = torch.device("cuda", 0)
     stream = torch.cuda.current_stream(dev)
     T = lambda x: torch.tensor(x, device=dev)  # noqa: E731
@@ -212,7 +216,8 @@ def main():
         ms = s.elapsed_time(e)
         print(json.dumps({"case": a.case, "launch": k, "ms": ms, "orbit_steps_per_s": n * a.nsteps / (ms * 1e-3),
                           "lanes": a.lanes, "block": a.block or 128, "orbits": n, "nsteps": a.nsteps,
-                          "division": sim.division, "min_blocks": a.min_blocks}), flush=True)
+                          "division": sim.division, "min_blocks": a.min_blocks,
+                          "record_store": a.record_store}), flush=True)
     sim.close()
 
 

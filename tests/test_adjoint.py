@@ -141,8 +141,11 @@ def test_adjoint_against_finite_differences_and_checkpoint_spacing():
     dev = torch.device("cuda")
     T = lambda a: torch.tensor(a, device=dev)  # noqa: E731
     sim = Integrator(system_path("oculomotor"), "rk4", orbits=n, **kw)
-    grads = [Adjoint(sim, ckpt_every=c)(T(t0), T(y0), T(p), T(tg)) for c in (0, 1, 7, 500)]
-    for g in grads[1:]:  # recomputation is exact: same gradients for any spacing
+    # 500 steps: ckpt_every 500 and above leave one segment, recorded by the
+    # forward sweep itself (no recomputation)
+    grads = [Adjoint(sim, ckpt_every=c)(T(t0), T(y0), T(p), T(tg)) for c in (0, 1, 7, 499, 500, 10**6)]
+    for g in grads[1:]:  # recomputation is exact: same loss and gradients for any spacing
+        assert torch.equal(g[0], grads[0][0])
         assert torch.equal(g[1], grads[0][1]) and torch.equal(g[2], grads[0][2])
     wide = Integrator(system_path("oculomotor"), "rk4", orbits=n * 24, **kw)
     fd_p, fd_y = finite_difference_gradient(T(t0), T(y0), T(p), T(tg), Adjoint(wide))

@@ -399,6 +399,70 @@ def test_implicit_kernel_launch_shapes_agree(solver):
         np.testing.assert_array_equal(rec[:, :, lo:hi].cpu().numpy(), outs[0][0][:, :, lo:hi])
 
 
+def test_pair_stores_write_the_same_records():
+    """Paired record stores (neighbouring orbits swap values and each writes
+    one equation of both as a vector store) give the records of direct
+    stores bit for bit: even and odd orbit counts (a last orbit without a
+    partner), a block size that is odd (direct stores throughout), an odd
+    equation count (the last equation stored alone), FP32 compute and, through
+    sodecl_cuda_launch, an odd first column, an odd row stride, a record base
+    off the 16-byte grid and float records."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    kw = dict(dt=1e-3, tspan=30e-3, ksteps=10, neq=6, npar=6)
+    for n in (1, 2, 33, 1000, 4097):
+        t0, y0, p = oculomotor_inputs(n, 40 + n)
+        for solver, block, prec in (("rk4", 128, "fp64"), ("rk4", 33, "fp64"), ("euler", 64, "fp64"),
+                                    ("rk4", 128, "fp32")):
+            outs = []
+            for store in ("direct", "pairs"):
+                with Integrator(system_path("oculomotor"), solver, orbits=n, block=block, precision=prec,
+                                record_store=store, **kw) as sim:
+                    sim.upload(t0, y0, p)
+                    outs.append(sim.run())
+            np.testing.assert_array_equal(outs[1], outs[0])
+    # an odd equation count: Kuramoto with 5 phases
+    rng = np.random.default_rng(41)
+    n, N_osc = 1001, 5
+    p = np.concatenate([rng.uniform(0, 5, (n, 1)), np.tile(rng.normal(size=N_osc), (n, 1)),
+                        rng.uniform(0, 0.5, (n, N_osc))], axis=1)
+    y0 = rng.uniform(0, 2 * np.pi, (n, N_osc))
+    outs = []
+    for store in ("direct", "pairs"):
+        with Integrator(system_path("kuramoto"), "euler", orbits=n, dt=0.01, tspan=0.3, ksteps=10, neq=N_osc,
+                        npar=2 * N_osc + 1, record_store=store) as sim:
+            sim.upload(np.zeros(n), y0, p)
+            outs.append(sim.run())
+    np.testing.assert_array_equal(outs[1], outs[0])
+    # the device launch: column offsets, strides, bases and record types; every
+    # record of the orbit range is written (the fill is exact in float too)
+    FILL = -1234.5
+    n = 5000
+    t0, y0, p = oculomotor_inputs(n, 42)
+    T = lambda x: torch.tensor(x, device=dev)  # noqa: E731
+    for lo, stride_pad, base_off, f32 in ((1, 0, 0, False), (2, 1, 0, False), (0, 0, 1, False), (3, 0, 0, True),
+                                          (0, 0, 0, True)):
+        m = n - 7
+        stride = lo + m + stride_pad
+        outs = []
+        for store in ("direct", "pairs"):
+            with Integrator(system_path("oculomotor"), "rk4", orbits=n, record_store=store, record_f32=f32,
+                            **kw) as sim:
+                td, yd, pd = T(t0[:m]), T(y0[:m]), T(p[:m])
+                nchunks = sim.num_chunks
+                rec = torch.full(((nchunks + 1) * 6 * stride + base_off,), FILL,
+                                 dtype=torch.float32 if f32 else torch.float64, device=dev)
+                sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(),
+                           records=rec.data_ptr() + base_off * rec.element_size(), n=m, rec_stride=stride,
+                           rec_col0=lo, chunk_begin=0, chunk_end=nchunks, write_final=True,
+                           stream=torch.cuda.current_stream(dev).cuda_stream)
+                torch.cuda.synchronize()
+                outs.append(rec.cpu().numpy())
+        np.testing.assert_array_equal(outs[1], outs[0])
+        assert not (outs[0][base_off:].reshape(nchunks + 1, 6, stride)[:, :, lo:lo + m] == FILL).any()
+
+
 # --------------------------------------------------------------------------
 # the reciprocal quotient
 
