@@ -482,7 +482,12 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
     // forward: loss at every record, checkpoints every C steps; with one
     // segment (C >= steps) the sweep records the segment itself, and the
     // backward pass has nothing to recompute
+#if SODECL_ADJ_GRADIENT
     const bool whole = a.grad_p && C >= steps;
+#else
+    // the loss-only kernel: the forward sweep alone, nothing recorded
+    const bool whole = false;
+#endif
     double loss = 0.0;
     for (int s = 0; s <= steps; ++s) {
         if (s % _numsteps_ == 0) {
@@ -492,7 +497,7 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
                 loss += d * d;
             }
         }
-        if (a.grad_p && !whole && s % C == 0 && s < steps) {
+        if (SODECL_ADJ_GRADIENT && a.grad_p && !whole && s % C == 0 && s < steps) {
             const long long c = s / C;
             a.ckpt_t[c * n + i] = (double)t;
             for (int e = 0; e < _numeq_; ++e) a.ckpt[(c * _numeq_ + e) * n + i] = (double)y[e];
@@ -502,10 +507,11 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
                                 whole ? a.seg + (long long)s * SODECL_SEG_WIDTH * n + i : nullptr, n);
     }
     a.loss[i] = loss * w;
-    if (!a.grad_p) {
+    if (!SODECL_ADJ_GRADIENT || !a.grad_p) {
         if (a.flags) a.flags[i] = capped ? SODECL_FLAG_NEWTON_CAP : 0;
         return;
     }
+#if SODECL_ADJ_GRADIENT
 
     // backward, segment by segment from the last
 #if SODECL_ADJ_MODE != 0
@@ -557,5 +563,6 @@ extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS
     if (a.grad_y0)
         for (int e = 0; e < _numeq_; ++e) a.grad_y0[i * _numeq_ + e] = lambda[e];
     if (a.flags) a.flags[i] = (overflow ? SODECL_FLAG_TAPE_OVERFLOW : 0) | (capped ? SODECL_FLAG_NEWTON_CAP : 0);
+#endif  // SODECL_ADJ_GRADIENT
 }
 #endif  // SODECL_ADJOINT_KERNEL

@@ -593,7 +593,7 @@ std::string assemble_batch(const std::vector<BatchClass> &classes, bool fast_div
 }
 
 std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, int tape_cap, int mode,
-                             bool fast_div)
+                             bool fast_div, bool gradient)
 {
     const SystemTraits tr = inspect_system(src);
     std::ostringstream s;
@@ -608,6 +608,7 @@ std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, in
     if (spec.min_blocks > 0) s << "#define SODECL_MIN_BLOCKS " << spec.min_blocks << "\n";
     s << "#define SODECL_TAPE_CAP " << tape_cap << "\n";
     s << "#define SODECL_ADJ_MODE " << mode << "\n";
+    s << "#define SODECL_ADJ_GRADIENT " << (gradient ? 1 : 0) << "\n";
     s << kFastDivSrc << "\n" << kPreludeSrc << "\n" << kThreefrySrc << "\n" << kAdjointSrc << "\n";
     s << "#define _numnoi_ " << spec.num_noi << "\n";
     s << "#define _listsize_ " << spec.list_size << "\n";
@@ -635,17 +636,17 @@ std::string assemble_adjoint(const ProgramSpec &spec, const std::string &src, in
 }  // namespace
 
 std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std::string &system_src, int tape_cap,
-                                             int mode)
+                                             int mode, bool gradient)
 {
     // the reciprocal quotients only where the system file is plain arithmetic
     if (spec.fast_div && system_src.find("printf") == std::string::npos) {
         try {
-            return compile_text(assemble_adjoint(spec, system_src, tape_cap, mode, true), spec.fmad, true,
+            return compile_text(assemble_adjoint(spec, system_src, tape_cap, mode, true, gradient), spec.fmad, true,
                                 "sodecl_adjoint");
         } catch (const std::exception &) {
         }
     }
-    return compile_text(assemble_adjoint(spec, system_src, tape_cap, mode, false), spec.fmad, false,
+    return compile_text(assemble_adjoint(spec, system_src, tape_cap, mode, false, gradient), spec.fmad, false,
                         "sodecl_adjoint");
 }
 

@@ -81,9 +81,10 @@ std::shared_ptr<const Program> build(const ProgramSpec &spec, const std::string 
 // solver: the system file twice, plain and with `double` recording on a tape
 // of `tape_cap` entries per right-hand-side evaluation.  mode: where the
 // vector-Jacobian products come from -- 2 the file's calc_vjp, 1 its
-// calc_jacobian and calc_jacobian_params, 0 the tape.
+// calc_jacobian and calc_jacobian_params, 0 the tape.  gradient = false
+// builds the loss-only kernel (the forward sweep alone).
 std::shared_ptr<const Program> build_adjoint(const ProgramSpec &spec, const std::string &system_src, int tape_cap,
-                                             int mode);
+                                             int mode, bool gradient = true);
 
 // One class of a heterogeneous batch: a system file with a solver, sizes,
 // step and Newton settings (kernel_steps/list_size unused).

@@ -133,6 +133,7 @@ struct sodecl_ctx {
     int adj_tape = 0;
     int adj_mode = -1;
     bool adj_fast_div = false;
+    bool adj_gradient = false;
     void *adj_scratch = nullptr;
     size_t adj_scratch_bytes = 0;
 
@@ -1109,13 +1110,13 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     // quotients are the same either way.
     const bool fast_div = !with_gradient && reciprocal_division(ctx->cfg);
     if (!ctx->adj_prog || ctx->adj_tape != tape || ctx->adj_mode != mode || ctx->adj_min_blocks != min_blocks ||
-        ctx->adj_fast_div != fast_div || ctx->adj_block != block) {
+        ctx->adj_fast_div != fast_div || ctx->adj_block != block || ctx->adj_gradient != with_gradient) {
         try {
             ProgramSpec spec = make_spec(ctx->cfg);
             spec.block_max = block;
             spec.min_blocks = min_blocks;
             spec.fast_div = fast_div;
-            auto prog = sodecl_b200::build_adjoint(spec, ctx->system_src, tape, mode);
+            auto prog = sodecl_b200::build_adjoint(spec, ctx->system_src, tape, mode, with_gradient);
             if (ctx->adj_lib) cudaLibraryUnload(ctx->adj_lib);
             ctx->adj_lib = nullptr;
             ctx->adj_kernel = nullptr;
@@ -1125,6 +1126,7 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
             ctx->adj_min_blocks = min_blocks;
             ctx->adj_fast_div = fast_div;
             ctx->adj_block = block;
+            ctx->adj_gradient = with_gradient;
         } catch (const std::exception &ex) {
             return ctx->fail(SODECL_ERR_COMPILE, ex.what());
         }
@@ -1150,18 +1152,22 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     // (0.70x the time at 2^16 orbits x 5000 RK4 steps) -- when its buffer
     // takes at most half the device's free memory (or what the context
     // already holds), else ceil(sqrt(steps)) as the memory-lean schedule.
+    // (The free-memory query can take milliseconds, so it is made only when
+    // the context does not hold a large enough buffer already.)
     int C = io->ckpt_every;
     if (C <= 0) {
         C = std::max<int>(1, static_cast<int>(std::ceil(std::sqrt(static_cast<double>(steps)))));
         const double whole_bytes = 8.0 * n * (static_cast<double>(steps) * seg_width + neq + 1);
-        size_t free_b = 0, total_b = 0;
-        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
-            cudaGetLastError();
-            free_b = 0;
+        bool whole = with_gradient && steps > 0 && whole_bytes <= static_cast<double>(ctx->adj_scratch_bytes);
+        if (with_gradient && steps > 0 && !whole) {
+            size_t free_b = 0, total_b = 0;
+            if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+                cudaGetLastError();
+                free_b = 0;
+            }
+            whole = whole_bytes <= 0.5 * static_cast<double>(free_b);
         }
-        if (steps > 0 && (whole_bytes <= 0.5 * static_cast<double>(free_b) ||
-                          whole_bytes <= static_cast<double>(ctx->adj_scratch_bytes)))
-            C = static_cast<int>(steps);
+        if (whole) C = static_cast<int>(steps);
     }
     if (steps > 0 && C > steps) C = static_cast<int>(steps);
     const int64_t nckpt = steps > 0 ? (steps + C - 1) / C : 1;
