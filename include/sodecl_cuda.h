@@ -197,6 +197,11 @@ void sodecl_cuda_destroy(sodecl_ctx *ctx);
 const char *sodecl_cuda_strerror(int status);
 int sodecl_cuda_abi_version(void);
 int sodecl_cuda_device_count(int *count);
+/* The device's name and compute capability ("NVIDIA B200", 10, 0); the name
+ * is copied NUL-terminated into buf (up to n bytes; buf may be NULL).  For the
+ * manager's log file; the reference's choose_device logs its OpenCL
+ * device's name and version (src/sodeclmgr.cpp:195-205). */
+int sodecl_cuda_device_describe(int device, char *buf, size_t n, int *major, int *minor);
 
 /* ---- device-buffer path (torch / custom callers; no host copies) ------- */
 

@@ -10,6 +10,7 @@
 #define SODECL_B200_SODECLMGR_HPP
 
 #include <cstdint>
+#include <sstream>
 #include <string>
 #include <vector>
 
@@ -40,7 +41,11 @@ class sodeclmgr {
     int64_t m_output_size = 0;
 
     // kernel_path_str is accepted and ignored (the solvers are built in);
-    // sode_system_str is the path of the system file, read at setup.
+    // sode_system_str is the path of the system file, read at setup.  As the
+    // reference's manager does, construction starts sodecllog.txt and
+    // sodeclexitstatus.txt empty in the working directory, each run appends
+    // its log lines to the first, and destruction appends "1 Normal." to the
+    // second.
     sodeclmgr(std::string kernel_path_str, char *sode_system_str, solver_Type solver, double dt, double int_time,
               int kernel_steps, int num_equat, int num_params, int num_noi, int list_size, output_Type output_type);
     ~sodeclmgr();
@@ -96,6 +101,10 @@ class sodeclmgr {
     const double *m_counters = nullptr;
     sodecl_ctx *m_ctx = nullptr;
     std::string m_error;
+    // What the reference's log singleton collects (src/clog.cpp): appended
+    // to sodecllog.txt in the working directory after each run.
+    std::ostringstream m_log;
+    void flush_log();
 };
 
 }  // namespace sodecl

@@ -499,6 +499,27 @@ const char *sodecl_cuda_strerror(int status)
     }
 }
 
+int sodecl_cuda_device_describe(int device, char *buf, size_t n, int *major, int *minor)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return SODECL_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        cudaGetLastError();
+        return SODECL_ERR_CUDA;
+    }
+    if (buf && n > 0) {
+        std::strncpy(buf, prop.name, n - 1);
+        buf[n - 1] = '\0';
+    }
+    if (major) *major = prop.major;
+    if (minor) *minor = prop.minor;
+    return SODECL_OK;
+}
+
 int sodecl_cuda_device_count(int *count)
 {
     if (!count) return SODECL_ERR_INVALID_ARG;

@@ -36,9 +36,25 @@ sodeclmgr::sodeclmgr(std::string kernel_path_str, char *sode_system_str, solver_
     m_cfg.num_params = num_params;
     m_cfg.num_noi = num_noi;
     m_cfg.list_size = list_size;
+    // the log files start empty (src/clog.cpp:22-28)
+    std::ofstream("sodecllog.txt", std::ios::binary | std::ios::out);
+    std::ofstream("sodeclexitstatus.txt", std::ios::binary | std::ios::out);
 }
 
-sodeclmgr::~sodeclmgr() { sodecl_cuda_destroy(m_ctx); }
+sodeclmgr::~sodeclmgr()
+{
+    sodecl_cuda_destroy(m_ctx);
+    // a normal exit (src/sodeclmgr.cpp:146-147, src/clog.cpp:76-92)
+    std::ofstream f("sodeclexitstatus.txt", std::ios::binary | std::ios::app | std::ios::out);
+    f << "1 Normal.";
+}
+
+void sodeclmgr::flush_log()
+{
+    std::ofstream f("sodecllog.txt", std::ios::binary | std::ios::app | std::ios::out);
+    f << m_log.str();
+    m_log.str(std::string());
+}
 
 int sodeclmgr::choose_device(unsigned platform_num, device_Type device_type, unsigned device_num)
 {
@@ -50,6 +66,14 @@ int sodeclmgr::choose_device(unsigned platform_num, device_Type device_type, uns
         return 0;
     }
     m_cfg.device = static_cast<int>(device_num);
+    // the selected device, as src/sodeclmgr.cpp:195-205 logs its OpenCL device
+    char name[256] = {0};
+    int major = 0, minor = 0;
+    if (sodecl_cuda_device_describe(m_cfg.device, name, sizeof name, &major, &minor) == SODECL_OK) {
+        m_log << "Selected platform name: NVIDIA CUDA\n";
+        m_log << "Selected device name: " << name << "\n";
+        m_log << "Selected device compute capability: " << major << "." << minor << "\n";
+    }
     return 1;
 }
 
@@ -130,6 +154,10 @@ int sodeclmgr::setup_sode_solver()
         std::ofstream dump("Generated_kernel.cl");
         dump << program;
     }
+    // the files the program was built from and how (src/sodeclmgr.cpp:459-460, :579-581)
+    m_log << m_system_path << "\n";
+    m_log << "Build options string: NVRTC --gpu-architecture=sm_100a --fmad=" << (m_cfg.fmad ? "true" : "false")
+          << "\n";
     rc = sodecl_cuda_upload(m_ctx, m_t0, m_y0, m_params, m_counters);
     if (rc != SODECL_OK) {
         m_error = ctx_error(m_ctx);
@@ -143,6 +171,7 @@ int sodeclmgr::run_sode_solver()
 {
     if (!m_ctx) return 0;
     const int64_t per_run = sodecl_cuda_num_records(m_ctx) * m_cfg.num_equat * m_cfg.list_size;
+    m_log << "The local group size is: " << static_cast<double>(m_cfg.local_group_size) << "\n";
     const auto start = std::chrono::steady_clock::now();
     int rc;
     if (m_output_type == output_Type::None) {
@@ -164,11 +193,15 @@ int sodeclmgr::run_sode_solver()
     if (rc != SODECL_OK) {
         m_error = ctx_error(m_ctx);
         std::cout << "Error: failed to run the solver: " << m_error << std::endl;
+        m_log << "Error: Failed to execute kernel!" << m_error;
+        flush_log();
         return 0;
     }
     m_output_size = static_cast<int64_t>(m_output.size());
     const double walltime = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
     std::cout << "Compute results runtime: " << walltime << " sec.\n";
+    m_log << "Compute results runtime: " << walltime << "sec.\n";  // src/sodeclmgr.cpp:1019-1029
+    flush_log();
     return 1;
 }
 
@@ -180,14 +213,19 @@ int64_t sodeclmgr::output_length() const
 int sodeclmgr::run_sode_solver_into(double *out, int64_t out_len)
 {
     if (!m_ctx) return 0;
+    m_log << "The local group size is: " << static_cast<double>(m_cfg.local_group_size) << "\n";
     const auto start = std::chrono::steady_clock::now();
     if (sodecl_cuda_run(m_ctx, out, out_len) != SODECL_OK) {
         m_error = ctx_error(m_ctx);
         std::cout << "Error: failed to run the solver: " << m_error << std::endl;
+        m_log << "Error: Failed to execute kernel!" << m_error;
+        flush_log();
         return 0;
     }
     const double walltime = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
     std::cout << "Compute results runtime: " << walltime << " sec.\n";
+    m_log << "Compute results runtime: " << walltime << "sec.\n";
+    flush_log();
     return 1;
 }
 

@@ -221,14 +221,24 @@ def test_reference_system_files_compile_unchanged(path, solvers):
         N.lib.sodecl_cuda_destroy(ctx)
 
 
-def test_python_module_fails_cleanly_without_device():
+def test_python_module_fails_cleanly_without_device(tmp_path, monkeypatch):
+    """Without a device the call returns an empty list.  The manager still
+    leaves the reference's side effects in the working directory: the
+    assembled program (built without a GPU), sodecllog.txt (started empty; no
+    run, so nothing appended) and sodeclexitstatus.txt with the normal-exit
+    line its destructor writes."""
     from sodecl_b200 import sodecl_interface
 
     if N.device_count() > 0:
         pytest.skip("checks the no-device path")
+    monkeypatch.chdir(tmp_path)
+    (tmp_path / "sodecllog.txt").write_text("left over from an earlier call")
     out = sodecl_interface.sodeclcall([0.0], [0, 0, 0, 0, 0, 2.0], [120, 1.5, 0.0045, 0.05, 600, 9.0], 0, 0,
                                       system_path("oculomotor"), 2, 1, 6, 6, 0, 1e-3, 0.01, 10, 0)
     assert out == []
+    assert (tmp_path / "Generated_kernel.cl").read_text().startswith("// SODECL program generated")
+    assert (tmp_path / "sodecllog.txt").read_text() == ""
+    assert (tmp_path / "sodeclexitstatus.txt").read_text() == "1 Normal."
     out = sodecl_interface.sodeclcall([0.0], [0.0] * 6, [1.0] * 6, 0, 0, system_path("oculomotor"), 9, 1, 6, 6, 0,
                                       1e-3, 0.01, 10, 0)
     assert out == []

@@ -83,6 +83,12 @@ def test_reference_known_answer_tests_run_unmodified(tmp_path):
     print(out.stdout[-4000:], out.stderr[-4000:])
     assert out.returncode == 0
     assert "Ran 4 tests" in out.stderr and "OK" in out.stderr.splitlines()[-1]
+    # the manager's side effects in the working directory, as the reference
+    # leaves them: the last call's log and its normal-exit line
+    log = (work / "sodecllog.txt").read_text()
+    assert "Selected device name: " in log and "Compute results runtime: " in log
+    assert (work / "sodeclexitstatus.txt").read_text() == "1 Normal."
+    assert (work / "Generated_kernel.cl").is_file()
 
 
 def oculomotor_case(solver, n, seed):
