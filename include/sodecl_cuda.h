@@ -126,7 +126,9 @@ typedef struct sodecl_cfg {
                                 warp) or SODECL_STORE_PAIRS (neighbouring orbits swap values
                                 with a shuffle and each writes one equation of both as a
                                 16-byte store).  Same records either way; the tuner times both.
-                                No counterpart in the reference. */
+                                One thread per orbit with the Euler, RK4 and Euler-Maruyama
+                                solvers only (elsewhere the direct stores run).  No
+                                counterpart in the reference. */
 } sodecl_cfg;
 
 #define SODECL_STORE_DIRECT 0

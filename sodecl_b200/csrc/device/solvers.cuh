@@ -34,14 +34,17 @@
 #ifndef SODECL_MIN_BLOCKS
 #define SODECL_MIN_BLOCKS 1
 #endif
-#ifndef SODECL_PAIR_STORES
-#define SODECL_PAIR_STORES 0
-#endif
 template <class T> struct sodecl_pair_of;
 template <> struct sodecl_pair_of<double> { typedef double2 type; };
 template <> struct sodecl_pair_of<float> { typedef float2 type; };
 #ifndef SODECL_LANES
 #define SODECL_LANES 1
+#endif
+#ifndef SODECL_PAIR_STORES
+#define SODECL_PAIR_STORES 0
+#endif
+#if SODECL_PAIR_STORES && (SODECL_LANES != 1 || SODECL_SOLVER > 2)
+#error "paired record stores serve the one-thread kernel of the explicit and stochastic solvers"
 #endif
 
 #if SODECL_RECORD_F32

@@ -452,7 +452,13 @@ ProgramSpec make_spec(const sodecl_cfg &c)
         spec.min_blocks = std::max(1, 65536 / (spec.block_max * 85));
     spec.fast_div = reciprocal_division(c);
     spec.lanes = lanes_of(c);
-    spec.pair_stores = c.record_store == SODECL_STORE_PAIRS && spec.lanes == 1;
+    // paired stores need the pair's two threads at the same store with orbits
+    // 2k and 2k+1: the one-thread kernel of the explicit and stochastic
+    // solvers (the implicit and adaptive kernels store per lane, whenever that
+    // lane's orbit reaches a record)
+    spec.pair_stores = c.record_store == SODECL_STORE_PAIRS && spec.lanes == 1 &&
+                       (c.solver == SODECL_EULER || c.solver == SODECL_RUNGE_KUTTA ||
+                        c.solver == SODECL_STOCHASTIC_EULER);
     spec.rtol = c.rtol;
     spec.atol = c.atol;
     spec.max_steps = c.max_steps;
@@ -1037,7 +1043,8 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
         }
     }
     // the winner with paired record stores (one thread per orbit)
-    if (rc == SODECL_OK && rec && pick.lanes == 1 && best < 1e300) {
+    if (rc == SODECL_OK && rec && pick.lanes == 1 && best < 1e300 &&
+        (solver == SODECL_EULER || solver == SODECL_RUNGE_KUTTA || solver == SODECL_STOCHASTIC_EULER)) {
         Cand c = pick;
         c.store = SODECL_STORE_PAIRS;
         float ms = 0.f;

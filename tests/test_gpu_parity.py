@@ -422,6 +422,18 @@ def test_pair_stores_write_the_same_records():
                     sim.upload(t0, y0, p)
                     outs.append(sim.run())
             np.testing.assert_array_equal(outs[1], outs[0])
+    # the implicit and adaptive kernels hand orbits to lanes out of order and
+    # store per lane: they keep the direct stores whatever is asked
+    n = 1000
+    t0, y0, p = oculomotor_inputs(n, 43)
+    for solver in ("ie", "im", "dp45"):
+        outs = []
+        for store in ("direct", "pairs"):
+            with Integrator(system_path("oculomotor"), solver, orbits=n, record_store=store, **kw) as sim:
+                assert "SODECL_PAIR_STORES" not in sim.program_source
+                sim.upload(t0, y0, p)
+                outs.append(sim.run())
+        np.testing.assert_array_equal(outs[1], outs[0])
     # an odd equation count: Kuramoto with 5 phases
     rng = np.random.default_rng(41)
     n, N_osc = 1001, 5
