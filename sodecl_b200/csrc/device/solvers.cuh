@@ -327,104 +327,123 @@ __device__ __forceinline__ void sodecl_step_em(real_t h, real_t t, real_t *y, re
 // Equations I", II.4).  No counterpart in the reference, which lists
 // variable-step solvers as future work.
 //
-// sodecl_dp_interval integrates the orbit from t to t + span (one record
-// interval), the last step cut to land on it exactly.  A step of size hh is
-// accepted when the RMS over equations of e_i / (atol + rtol max(|y_i|, |y5_i|))
-// is at most 1 (e the difference of the embedded 5th- and 4th-order results);
-// the next step is hh * min(5, max(0.2, 0.9 err^(-1/5))), not larger than hh
-// after a rejection; a step cut to the interval's end leaves the proposal `h`
-// as it was.  The first stage is re-evaluated at each interval's start, so
-// results do not depend on how intervals are grouped into launches.  Returns
-// false (state NaN) when the interval needs more than SODECL_MAX_STEPS
-// attempts or a step too small to advance t.
+// The adaptive solver integrates each record interval [t, t + span) in
+// attempted steps, the last cut to land on the interval's end exactly.  A
+// step of size hh is accepted when the RMS over equations of
+// e_i / (atol + rtol max(|y_i|, |y5_i|)) is at most 1 (e the difference of
+// the embedded 5th- and 4th-order results); the next step is
+// hh * min(5, max(0.2, 0.9 err^(-1/5))), not larger than hh after a
+// rejection; a step cut to the interval's end leaves the proposal `h` as it
+// was.  The first stage is re-evaluated at each interval's start, so results
+// do not depend on how intervals are grouped into launches.  An interval that
+// needs more than SODECL_MAX_STEPS attempts, or a step too small to advance
+// t, fails: the state becomes NaN.
 #define SODECL_DP(c) ((real_t)(c))
-__device__ __forceinline__ bool sodecl_dp_interval(real_t &t, real_t *y, real_t *p, real_t &h, const real_t span,
-                                                   sodecl_i64 &accepted)
+struct sodecl_dp_state {
+    real_t k1[_numeq_];  // the first stage at (t, y) (first same as last)
+    real_t t_end;        // the interval's end
+    int n;               // attempts in this interval
+    bool rejected;       // the last attempt was rejected
+};
+
+// Opens the interval of length span from t.  Returns false when it needs no
+// attempt: a diverged orbit stays as it is (t moves to the interval's end),
+// and an interval too short to advance t ends at once.
+__device__ __forceinline__ bool sodecl_dp_begin(real_t &t, const real_t *y, real_t *p, real_t &h, const real_t span,
+                                                sodecl_dp_state &st)
 {
-    real_t k1[_numeq_], k2[_numeq_], k3[_numeq_], k4[_numeq_], k5[_numeq_], k6[_numeq_], k7[_numeq_];
-    real_t yt[_numeq_], y5[_numeq_];
-    const real_t t_end = t + span;
+    st.t_end = t + span;
     bool finite = true;
 #pragma unroll SODECL_EQ_UNROLL
     for (int e = 0; e < _numeq_; ++e) finite = finite && isfinite(y[e]);
-    if (!finite) {  // a diverged orbit stays as it is
-        t = t_end;
-        return true;
+    if (!finite) {
+        t = st.t_end;
+        return false;
     }
     if (!(h > (real_t)0) || !isfinite(h)) h = (real_t)_m_dt_;
-    sode_system(t, y, k1, p);
-    bool rejected = false;
-#pragma unroll 1
-    for (int n = 0; t < t_end; ++n) {
-        if (n >= SODECL_MAX_STEPS) break;
-        const bool last = t + h >= t_end;
-        const real_t hh = last ? t_end - t : h;
-        if (!(hh > (real_t)0) || t + hh == t) break;
-#pragma unroll SODECL_EQ_UNROLL
-        for (int e = 0; e < _numeq_; ++e) yt[e] = y[e] + hh * (SODECL_DP(1.0 / 5.0) * k1[e]);
-        sode_system(t + SODECL_DP(1.0 / 5.0) * hh, yt, k2, p);
-#pragma unroll SODECL_EQ_UNROLL
-        for (int e = 0; e < _numeq_; ++e)
-            yt[e] = y[e] + hh * (SODECL_DP(3.0 / 40.0) * k1[e] + SODECL_DP(9.0 / 40.0) * k2[e]);
-        sode_system(t + SODECL_DP(3.0 / 10.0) * hh, yt, k3, p);
-#pragma unroll SODECL_EQ_UNROLL
-        for (int e = 0; e < _numeq_; ++e)
-            yt[e] = y[e] + hh * (SODECL_DP(44.0 / 45.0) * k1[e] + SODECL_DP(-56.0 / 15.0) * k2[e] +
-                                 SODECL_DP(32.0 / 9.0) * k3[e]);
-        sode_system(t + SODECL_DP(4.0 / 5.0) * hh, yt, k4, p);
-#pragma unroll SODECL_EQ_UNROLL
-        for (int e = 0; e < _numeq_; ++e)
-            yt[e] = y[e] + hh * (SODECL_DP(19372.0 / 6561.0) * k1[e] + SODECL_DP(-25360.0 / 2187.0) * k2[e] +
-                                 SODECL_DP(64448.0 / 6561.0) * k3[e] + SODECL_DP(-212.0 / 729.0) * k4[e]);
-        sode_system(t + SODECL_DP(8.0 / 9.0) * hh, yt, k5, p);
-#pragma unroll SODECL_EQ_UNROLL
-        for (int e = 0; e < _numeq_; ++e)
-            yt[e] = y[e] + hh * (SODECL_DP(9017.0 / 3168.0) * k1[e] + SODECL_DP(-355.0 / 33.0) * k2[e] +
-                                 SODECL_DP(46732.0 / 5247.0) * k3[e] + SODECL_DP(49.0 / 176.0) * k4[e] +
-                                 SODECL_DP(-5103.0 / 18656.0) * k5[e]);
-        sode_system(t + hh, yt, k6, p);
-#pragma unroll SODECL_EQ_UNROLL
-        for (int e = 0; e < _numeq_; ++e)
-            y5[e] = y[e] + hh * (SODECL_DP(35.0 / 384.0) * k1[e] + SODECL_DP(500.0 / 1113.0) * k3[e] +
-                                 SODECL_DP(125.0 / 192.0) * k4[e] + SODECL_DP(-2187.0 / 6784.0) * k5[e] +
-                                 SODECL_DP(11.0 / 84.0) * k6[e]);
-        sode_system(t + hh, y5, k7, p);
-        real_t acc = 0;
-#pragma unroll SODECL_EQ_UNROLL
-        for (int e = 0; e < _numeq_; ++e) {
-            const real_t err = hh * (SODECL_DP(71.0 / 57600.0) * k1[e] + SODECL_DP(-71.0 / 16695.0) * k3[e] +
-                                     SODECL_DP(71.0 / 1920.0) * k4[e] + SODECL_DP(-17253.0 / 339200.0) * k5[e] +
-                                     SODECL_DP(22.0 / 525.0) * k6[e] + SODECL_DP(-1.0 / 40.0) * k7[e]);
-            const real_t sc = SODECL_DP(SODECL_ATOL) + SODECL_DP(SODECL_RTOL) * fmax(fabs(y[e]), fabs(y5[e]));
-            const real_t q = err / sc;
-            acc = acc + q * q;
-        }
-        const real_t err = sqrt(acc / (real_t)_numeq_);
-        real_t fac = (err > (real_t)0) ? SODECL_DP(0.9) * exp(SODECL_DP(-0.2) * log(err)) : SODECL_DP(5.0);
-        fac = fmin(SODECL_DP(5.0), fmax(SODECL_DP(0.2), fac));
-        if (err <= (real_t)1) {
-            t = last ? t_end : t + hh;
-#pragma unroll SODECL_EQ_UNROLL
-            for (int e = 0; e < _numeq_; ++e) {
-                y[e] = y5[e];
-                k1[e] = k7[e];
-            }
-            ++accepted;
-            if (!last) h = hh * (rejected ? fmin((real_t)1, fac) : fac);
-            rejected = false;
-        } else {
-            // a NaN error shrinks the step too
-            h = hh * (err == err ? fmin((real_t)1, fac) : SODECL_DP(0.2));
-            rejected = true;
-        }
-    }
-    if (t < t_end) {
+    sode_system(t, const_cast<real_t *>(y), st.k1, p);
+    st.n = 0;
+    st.rejected = false;
+    return t < st.t_end;
+}
+
+// One attempted step of the open interval.  Returns 0 while the interval
+// goes on, 1 when it has reached its end, 2 when it failed (state NaN, t at
+// the interval's end).
+__device__ __forceinline__ int sodecl_dp_attempt(real_t &t, real_t *y, real_t *p, real_t &h, sodecl_dp_state &st,
+                                                 sodecl_i64 &accepted)
+{
+    real_t k2[_numeq_], k3[_numeq_], k4[_numeq_], k5[_numeq_], k6[_numeq_], k7[_numeq_];
+    real_t yt[_numeq_], y5[_numeq_];
+    const real_t t_end = st.t_end;
+    const bool last = t + h >= t_end;
+    const real_t hh = last ? t_end - t : h;
+    if (st.n >= SODECL_MAX_STEPS || !(hh > (real_t)0) || t + hh == t) {
 #pragma unroll SODECL_EQ_UNROLL
         for (int e = 0; e < _numeq_; ++e) y[e] = (real_t)__longlong_as_double(0x7ff8000000000000ULL);
         t = t_end;
-        return false;
+        return 2;
     }
-    return true;
+    real_t *k1 = st.k1;
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) yt[e] = y[e] + hh * (SODECL_DP(1.0 / 5.0) * k1[e]);
+    sode_system(t + SODECL_DP(1.0 / 5.0) * hh, yt, k2, p);
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e)
+        yt[e] = y[e] + hh * (SODECL_DP(3.0 / 40.0) * k1[e] + SODECL_DP(9.0 / 40.0) * k2[e]);
+    sode_system(t + SODECL_DP(3.0 / 10.0) * hh, yt, k3, p);
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e)
+        yt[e] = y[e] + hh * (SODECL_DP(44.0 / 45.0) * k1[e] + SODECL_DP(-56.0 / 15.0) * k2[e] +
+                             SODECL_DP(32.0 / 9.0) * k3[e]);
+    sode_system(t + SODECL_DP(4.0 / 5.0) * hh, yt, k4, p);
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e)
+        yt[e] = y[e] + hh * (SODECL_DP(19372.0 / 6561.0) * k1[e] + SODECL_DP(-25360.0 / 2187.0) * k2[e] +
+                             SODECL_DP(64448.0 / 6561.0) * k3[e] + SODECL_DP(-212.0 / 729.0) * k4[e]);
+    sode_system(t + SODECL_DP(8.0 / 9.0) * hh, yt, k5, p);
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e)
+        yt[e] = y[e] + hh * (SODECL_DP(9017.0 / 3168.0) * k1[e] + SODECL_DP(-355.0 / 33.0) * k2[e] +
+                             SODECL_DP(46732.0 / 5247.0) * k3[e] + SODECL_DP(49.0 / 176.0) * k4[e] +
+                             SODECL_DP(-5103.0 / 18656.0) * k5[e]);
+    sode_system(t + hh, yt, k6, p);
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e)
+        y5[e] = y[e] + hh * (SODECL_DP(35.0 / 384.0) * k1[e] + SODECL_DP(500.0 / 1113.0) * k3[e] +
+                             SODECL_DP(125.0 / 192.0) * k4[e] + SODECL_DP(-2187.0 / 6784.0) * k5[e] +
+                             SODECL_DP(11.0 / 84.0) * k6[e]);
+    sode_system(t + hh, y5, k7, p);
+    real_t acc = 0;
+#pragma unroll SODECL_EQ_UNROLL
+    for (int e = 0; e < _numeq_; ++e) {
+        const real_t err = hh * (SODECL_DP(71.0 / 57600.0) * k1[e] + SODECL_DP(-71.0 / 16695.0) * k3[e] +
+                                 SODECL_DP(71.0 / 1920.0) * k4[e] + SODECL_DP(-17253.0 / 339200.0) * k5[e] +
+                                 SODECL_DP(22.0 / 525.0) * k6[e] + SODECL_DP(-1.0 / 40.0) * k7[e]);
+        const real_t sc = SODECL_DP(SODECL_ATOL) + SODECL_DP(SODECL_RTOL) * fmax(fabs(y[e]), fabs(y5[e]));
+        const real_t q = err / sc;
+        acc = acc + q * q;
+    }
+    const real_t err = sqrt(acc / (real_t)_numeq_);
+    real_t fac = (err > (real_t)0) ? SODECL_DP(0.9) * exp(SODECL_DP(-0.2) * log(err)) : SODECL_DP(5.0);
+    fac = fmin(SODECL_DP(5.0), fmax(SODECL_DP(0.2), fac));
+    if (err <= (real_t)1) {
+        t = last ? t_end : t + hh;
+#pragma unroll SODECL_EQ_UNROLL
+        for (int e = 0; e < _numeq_; ++e) {
+            y[e] = y5[e];
+            k1[e] = k7[e];
+        }
+        ++accepted;
+        if (!last) h = hh * (st.rejected ? fmin((real_t)1, fac) : fac);
+        st.rejected = false;
+    } else {
+        // a NaN error shrinks the step too
+        h = hh * (err == err ? fmin((real_t)1, fac) : SODECL_DP(0.2));
+        st.rejected = true;
+    }
+    ++st.n;
+    return t < t_end ? 0 : 1;
 }
 #undef SODECL_DP
 #endif
@@ -975,6 +994,94 @@ sodecl_orbits(const sodecl_args a)
         }
     }
 }
+#elif SODECL_LANES == 1 && SODECL_SOLVER == 5
+// From record interval c on: stores record c and opens its interval; an
+// interval that needs no attempt ends at once and the next one follows.
+// Past the launch's last interval the orbit is written out and the lane is
+// free (returns false).
+__device__ __forceinline__ bool sodecl_dp_open(const sodecl_args &a, sodecl_i64 i, int &c, real_t &t, real_t *y,
+                                               real_t *p, real_t &h, sodecl_dp_state &st, int &flags,
+                                               sodecl_i64 accepted, int capped)
+{
+    const real_t span = (real_t)_numsteps_ * (real_t)_m_dt_;
+#pragma unroll 1
+    for (; c < a.chunk_end; ++c) {
+        if (a.records) sodecl_store_record(a, c, i, y, flags);
+        if (sodecl_dp_begin(t, y, p, h, span, st)) return true;
+    }
+    // the orbit's next step size rides in the counters array
+    sodecl_orbit_out(a, i, t, y, (double)h, accepted, capped, flags);
+    return false;
+}
+
+// The adaptive solver, one thread per orbit.  Orbits need very different
+// numbers of attempted steps per interval, so, as in the implicit kernel,
+// attempts drive the loop (a lane whose interval has ended records and opens
+// the next at the following attempt), and each warp owns a contiguous range
+// of the launch's orbits that its lanes take in turn (a ballot hands them out
+// in lane order) when their orbit is done.  Each orbit's arithmetic is that of
+// integrating it alone.
+extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS)
+sodecl_orbits(const sodecl_args a)
+{
+    const int lane = threadIdx.x % 32;
+    const int in_warp = min(32, (int)blockDim.x - (int)(threadIdx.x / 32) * 32);
+    const unsigned wmask = in_warp == 32 ? 0xffffffffu : (1u << in_warp) - 1u;
+    const sodecl_i64 warps_per_block = (blockDim.x + 31) / 32;
+    const sodecl_i64 nwarps = (sodecl_i64)gridDim.x * warps_per_block;
+    const sodecl_i64 w = (sodecl_i64)blockIdx.x * warps_per_block + threadIdx.x / 32;
+    sodecl_i64 next = sodecl_split(a.n, w, nwarps);
+    const sodecl_i64 hi = sodecl_split(a.n, w + 1, nwarps);
+
+    real_t y[_numeq_];
+    real_t p[SODECL_NPAR_ALLOC];
+    real_t t = 0, h = 0;
+    sodecl_dp_state st;
+    sodecl_i64 i = 0, accepted = 0;
+    int c = 0, flags = 0, capped = 0;
+    bool active = false;
+#pragma unroll 1
+    for (;;) {
+        // hand the range's next orbits to the idle lanes
+        const unsigned idle = __ballot_sync(wmask, !active);
+        if (idle != 0u && next < hi) {
+            const sodecl_i64 mine = next + __popc(idle & ((1u << lane) - 1u));
+            next += __popc(idle);
+            if (!active && mine < hi) {
+                i = mine;
+                t = (real_t)a.t[i];
+#pragma unroll SODECL_EQ_UNROLL
+                for (int e = 0; e < _numeq_; ++e) y[e] = (real_t)a.y[i * _numeq_ + e];
+#pragma unroll SODECL_PAR_UNROLL
+                for (int k = 0; k < _numpar_; ++k) p[k] = (real_t)__ldg(a.p + i * _numpar_ + k);
+                h = a.counters ? (real_t)a.counters[i] : (real_t)0;
+                c = a.chunk_begin;
+                flags = capped = 0;
+                accepted = 0;
+                active = sodecl_dp_open(a, i, c, t, y, p, h, st, flags, accepted, capped);
+            }
+        }
+        if (!__any_sync(wmask, active)) {
+            if (next >= hi) break;
+            continue;
+        }
+        // attempts, until a lane is idle while the range has orbits left, or
+        // every lane is done
+#pragma unroll 1
+        for (;;) {
+            if (active) {
+                const int r = sodecl_dp_attempt(t, y, p, h, st, accepted);
+                if (r != 0) {
+                    if (r == 2) capped = 1;
+                    ++c;
+                    active = sodecl_dp_open(a, i, c, t, y, p, h, st, flags, accepted, capped);
+                }
+            }
+            const unsigned now_idle = __ballot_sync(wmask, !active);
+            if (now_idle == wmask || (now_idle != 0u && next < hi)) break;
+        }
+    }
+}
 #elif SODECL_LANES == 1
 extern "C" __global__ void __launch_bounds__(SODECL_BLOCK_MAX, SODECL_MIN_BLOCKS)
 sodecl_orbits(const sodecl_args a)
@@ -1000,18 +1107,6 @@ sodecl_orbits(const sodecl_args a)
     double counter = 0.0;
 #endif
 
-#if SODECL_SOLVER == 5
-    // the orbit's next step size rides in the counters array
-    real_t h = a.counters ? (real_t)a.counters[i] : (real_t)0;
-    const real_t span = (real_t)_numsteps_ * (real_t)_m_dt_;
-#pragma unroll 1
-    for (int c = a.chunk_begin; c < a.chunk_end; ++c) {
-        if (a.records)
-            sodecl_store_record(a, c, i, y, flags);
-        if (!sodecl_dp_interval(t, y, p, h, span, passes)) capped = 1;
-    }
-    counter = (double)h;
-#else
 #pragma unroll 1
     for (int c = a.chunk_begin; c < a.chunk_end; ++c) {
         if (a.records)
@@ -1020,7 +1115,6 @@ sodecl_orbits(const sodecl_args a)
         for (int s = 0; s < _numsteps_; ++s)
             sodecl_advance(t, y, p, gid, counter, passes, capped);
     }
-#endif
     sodecl_orbit_out(a, i, t, y, counter, passes, capped, flags);
 }
 #else  // SODECL_LANES > 1

@@ -376,10 +376,12 @@ int launch_kernel(sodecl_ctx *ctx, cudaKernel_t kernel, const sodecl_cfg &c, con
 {
     if (a.n <= 0) return SODECL_OK;
     Geometry g = geometry(c, a.n);
-    if (lanes_of(c) == 1 && (c.solver == SODECL_IMPLICIT_EULER || c.solver == SODECL_IMPLICIT_MIDPOINT)) {
-        // the implicit kernel's warps share out ranges of orbits among their
-        // lanes: give every lane the same number of orbits, the fewest that
-        // fit the threads resident at once, and launch just the blocks for that
+    if (lanes_of(c) == 1 && (c.solver == SODECL_IMPLICIT_EULER || c.solver == SODECL_IMPLICIT_MIDPOINT ||
+                             c.solver == SODECL_DORMAND_PRINCE)) {
+        // the implicit and adaptive kernels' warps share out ranges of orbits
+        // among their lanes: give every lane the same number of orbits, the
+        // fewest that fit the threads resident at once, and launch just the
+        // blocks for that
         int per_sm = 0, dev = 0, sms = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, reinterpret_cast<const void *>(kernel), g.block,
                                                           0) != cudaSuccess ||

@@ -163,6 +163,33 @@ def test_gpu_split_runs_equal_one_run():
 
 
 @pytest.mark.gpu
+def test_gpu_launch_shapes_agree():
+    """The adaptive kernel's warps hand out ranges of orbits to their lanes,
+    and the host launches only the blocks that give each lane the fewest
+    orbits that fit the resident threads.  Block sizes that are not a multiple
+    of 32, more orbits than resident threads (several orbits a lane) and a
+    register cap all give each orbit the records, step sizes, accepted-step
+    counts and flags of integrating it alone, bit for bit."""
+    n = 150000
+    t0, y0, p = inputs(n, 8)
+    kw = dict(dt=1e-3, tspan=0.06, ksteps=20, neq=6, npar=6, rtol=1e-6, atol=1e-9)
+    outs = []
+    for block, minb in ((128, 0), (100, 0), (33, 0), (512, 0), (128, 2)):
+        rec, t, y, h, passes, flags = run_gpu(t0, y0, p, block=block, min_blocks=minb, **kw)
+        outs.append((rec, h, passes, flags))
+    for got in outs[1:]:
+        for x, want in zip(got, outs[0]):
+            np.testing.assert_array_equal(x, want)
+    # a few orbits alone
+    idx = [0, 1, 77, 4097, n - 1]
+    rec1, _, _, h1, passes1, flags1 = run_gpu(t0[idx], y0[idx], p[idx], **kw)
+    np.testing.assert_array_equal(rec1, outs[0][0][:, :, idx])
+    np.testing.assert_array_equal(h1, outs[0][1][idx])
+    np.testing.assert_array_equal(passes1, outs[0][2][idx])
+    np.testing.assert_array_equal(flags1, outs[0][3][idx])
+
+
+@pytest.mark.gpu
 def test_gpu_step_limit_and_fp32():
     n = 500
     t0, y0, p = inputs(n, 7)
