@@ -30,8 +30,10 @@ def sodecl(openclplatform, opencldevice, openclkernel, initx, params, sodesolver
     # t0 = 0 for every orbit; nparams from the first parameter row (sodecl.py:40-46)
     t0 = numpy.zeros(orbits)
     nparams = numpy.asarray(params)[0].size
-    initx = numpy.asarray(initx, dtype=numpy.float64).flatten()
-    params = numpy.asarray(params, dtype=numpy.float64).flatten()
+    # flattened in C order, as the reference's flatten() calls do
+    # (sodecl.py:44-46); ravel copies only what is not already contiguous
+    initx = numpy.ravel(numpy.asarray(initx, dtype=numpy.float64))
+    params = numpy.ravel(numpy.asarray(params, dtype=numpy.float64))
 
     # solver choice (sodecl.py:48-61): any noise forces Euler-Maruyama; an
     # unknown deterministic solver falls back to Euler
