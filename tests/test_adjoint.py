@@ -268,7 +268,7 @@ def test_gradient_fit_reduces_the_loss():
         loss = trajectory_mse(torch.exp(logp), y0t, t0t, tgt, adj)
         loss.sum().backward()
         opt.step()
-        losses.append(float(loss.sum()))
+        losses.append(float(loss.detach().sum()))
     print("fit: loss %.3e -> %.3e" % (losses[0], losses[-1]))
     assert np.isfinite(losses).all()
     assert losses[-1] < 0.5 * losses[0]  # measured: 87.1 -> 18.6
