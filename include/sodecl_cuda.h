@@ -70,7 +70,7 @@ extern "C" {
  * division outside [2^-500, 2^500) (FP32: [2^-60, 2^60)): the same quotient as
  * SODECL_DIV_IEEE bit for bit (NaN payloads aside).  SODECL_DIV_DEFAULT (what
  * sodecl_cfg_init sets) is the reciprocal form in FP64 and IEEE division in
- * FP32.  On the oculomotor RK4 workload in FP64 the reciprocal form is 2 %
+ * FP32 and for the adaptive solver.  On the oculomotor RK4 workload in FP64 the reciprocal form is 2 %
  * faster on converging orbits and 1.8x on diverged ones; in FP32 it gains on
  * diverged orbits and loses on converging ones.  sodecl_cuda_autotune measures
  * both for a given system file. */
@@ -106,11 +106,12 @@ typedef struct sodecl_cfg {
     int32_t newton_max_iter; /* implicit solvers' pass limit; default 1000 (ie.cl:69, im.cl:65) */
     int32_t record_f32;      /* device-API records stored as float (sodecl_cuda_launch only) */
     int32_t min_blocks_per_sm; /* launch-bounds occupancy hint for the compiler; 0 = default: none, except
-                                  with one thread per orbit for the implicit solvers, which are held to
-                                  128 registers a thread, and for FP64 RK4 on up to 8 equations, held
-                                  to 85 (1 lifts either) */
+                                  with one thread per orbit for the implicit and adaptive solvers,
+                                  which are held to 128 registers a thread, and for FP64 RK4 on up to
+                                  8 equations, held to 85 (1 lifts either) */
     int32_t division;        /* quotients: SODECL_DIV_DEFAULT (the default: reciprocal in FP64, IEEE in
-                                FP32), SODECL_DIV_RECIPROCAL or SODECL_DIV_IEEE;
+                                FP32 and for SODECL_DORMAND_PRINCE), SODECL_DIV_RECIPROCAL or
+                                SODECL_DIV_IEEE;
                                 both give the IEEE-rounded quotient bit for bit */
     int32_t lanes_per_orbit; /* 0 or 1 (default): one thread per orbit.  2, 4, 8, 16 or 32:
                                 that many lanes of a warp share an orbit, each evaluating

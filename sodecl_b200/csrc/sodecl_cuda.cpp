@@ -413,10 +413,14 @@ int launch(sodecl_ctx *ctx, const DeviceArgs &a, cudaStream_t stream)
 
 // SODECL_DIV_DEFAULT: the reciprocal form in FP64 (faster on converging and
 // diverged orbits alike), IEEE division in FP32 (the reciprocal form gains
-// only on diverged orbits there; the tuner times both)
+// only on diverged orbits there; the tuner times both) and for the adaptive
+// solver, whose error test divides by a new scale every attempt: there the
+// wrapper's registers cost more than it saves (2^20 oculomotor orbits over
+// 0.2 time units: 241 against 199 ms at 128 registers)
 bool reciprocal_division(const sodecl_cfg &c)
 {
-    return c.division == SODECL_DIV_RECIPROCAL || (c.division == SODECL_DIV_DEFAULT && c.precision == SODECL_FP64);
+    return c.division == SODECL_DIV_RECIPROCAL ||
+           (c.division == SODECL_DIV_DEFAULT && c.precision == SODECL_FP64 && c.solver != SODECL_DORMAND_PRINCE);
 }
 
 ProgramSpec make_spec(const sodecl_cfg &c)
@@ -441,8 +445,12 @@ ProgramSpec make_spec(const sodecl_cfg &c)
     // implicit solvers, one thread per orbit: by default at most 128 registers
     // a thread (four blocks of 128 threads on an SM); above that the Newton
     // pass's hoisted terms took more registers than the occupancy they cost
+    // The adaptive solver's kernel likewise: the oculomotor model at 2^20
+    // orbits over 0.2 time units took 199 ms at 128 registers against 212 ms
+    // uncapped (202 registers).
     if (spec.min_blocks == 0 && lanes_of(c) == 1 &&
-        (c.solver == SODECL_IMPLICIT_EULER || c.solver == SODECL_IMPLICIT_MIDPOINT))
+        (c.solver == SODECL_IMPLICIT_EULER || c.solver == SODECL_IMPLICIT_MIDPOINT ||
+         c.solver == SODECL_DORMAND_PRINCE))
         spec.min_blocks = std::max(1, 65536 / (spec.block_max * 128));
     // FP64 RK4 on small systems, one thread per orbit: by default at most 85
     // registers a thread (three blocks of 256).  Measured on the oculomotor
@@ -957,12 +965,14 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
     // lanes per orbit: up to the first power of two >= the equations
     const auto traits = sodecl_b200::inspect_system(ctx->system_src);
     const int solver = ctx->cfg.solver;
-    // implicit solvers and FP64 RK4 on small systems run under a register cap
-    // by default (min_blocks 0); 1 lifts it
-    if (solver == SODECL_IMPLICIT_EULER || solver == SODECL_IMPLICIT_MIDPOINT ||
+    // implicit and adaptive solvers and FP64 RK4 on small systems run under a
+    // register cap by default (min_blocks 0); 1 lifts it
+    if (solver == SODECL_IMPLICIT_EULER || solver == SODECL_IMPLICIT_MIDPOINT || solver == SODECL_DORMAND_PRINCE ||
         (solver == SODECL_RUNGE_KUTTA && ctx->cfg.precision == SODECL_FP64 && ctx->cfg.num_equat <= 8))
-        cands.push_back({128, 1, ctx->cfg.precision == SODECL_FP64 ? SODECL_DIV_RECIPROCAL : SODECL_DIV_IEEE, 1,
-                         SODECL_STORE_DIRECT});
+        cands.push_back({128, 1,
+                         ctx->cfg.precision == SODECL_FP64 && solver != SODECL_DORMAND_PRINCE ? SODECL_DIV_RECIPROCAL
+                                                                                             : SODECL_DIV_IEEE,
+                         1, SODECL_STORE_DIRECT});
     const bool row_ok = lanes_supported(traits, solver);
     if (row_ok) {
         for (int l = 2; l <= 32 && l / 2 < ctx->cfg.num_equat; l *= 2) {

@@ -245,7 +245,8 @@ def test_python_module_fails_cleanly_without_device(tmp_path, monkeypatch):
 
 
 def test_division_modes_and_fallback():
-    """The default: the reciprocal quotient in FP64, IEEE division in FP32;
+    """The default: the reciprocal quotient in FP64, IEEE division in FP32 and
+    for the adaptive solver;
     either precision builds the reciprocal form when asked.  A system file
     that needs the plain scalar (an implicit conversion) falls back to IEEE
     division."""
@@ -254,6 +255,8 @@ def test_division_modes_and_fallback():
     assert Integrator(system_path("oculomotor"), "rk4", **kw).division == "reciprocal"  # the default
     assert Integrator(system_path("oculomotor"), "rk4", division="ieee", **kw).division == "ieee"
     assert Integrator(system_path("oculomotor"), "rk4", precision="fp32", **kw).division == "ieee"  # the default
+    assert Integrator(system_path("oculomotor"), "dp45", **kw).division == "ieee"  # the default
+    assert Integrator(system_path("oculomotor"), "dp45", division="reciprocal", **kw).division == "reciprocal"
     assert Integrator(system_path("oculomotor"), "rk4", division="reciprocal", precision="fp32",
                       **kw).division == "reciprocal"
     assert Integrator(system_path("oculomotor"), "rk4", division="ieee", precision="fp32", **kw).division == "ieee"
