@@ -34,7 +34,8 @@
 extern "C" {
 #endif
 
-#define SODECL_CUDA_ABI_VERSION 3
+/* 4: sodecl_cfg gained record_store (after max_steps) */
+#define SODECL_CUDA_ABI_VERSION 4
 
 /* status codes */
 #define SODECL_OK 0

@@ -23,7 +23,7 @@ ERR_OUT_OF_MEMORY = -8
 ERR_UNSUPPORTED = -9
 
 # include/sodecl_cuda.h's SODECL_CUDA_ABI_VERSION, which the structures below follow
-ABI_VERSION = 3
+ABI_VERSION = 4
 STOCHASTIC_EULER, EULER, RUNGE_KUTTA, IMPLICIT_EULER, IMPLICIT_MIDPOINT, DORMAND_PRINCE = range(6)
 FP64, FP32 = 0, 1
 DIV_RECIPROCAL, DIV_IEEE, DIV_DEFAULT = 0, 1, 2

@@ -37,7 +37,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_abi_version_and_strerror():
-    assert N.lib.sodecl_cuda_abi_version() == N.ABI_VERSION == 3
+    assert N.lib.sodecl_cuda_abi_version() == N.ABI_VERSION == 4
     assert N.lib.sodecl_cuda_strerror(N.ERR_NO_JACOBIAN).decode().startswith("implicit solver")
 
 
