@@ -430,7 +430,7 @@ def test_pair_stores_write_the_same_records():
         outs = []
         for store in ("direct", "pairs"):
             with Integrator(system_path("oculomotor"), solver, orbits=n, record_store=store, **kw) as sim:
-                assert "SODECL_PAIR_STORES" not in sim.program_source
+                assert "#define SODECL_PAIR_STORES 1" not in sim.program_source
                 sim.upload(t0, y0, p)
                 outs.append(sim.run())
         np.testing.assert_array_equal(outs[1], outs[0])
