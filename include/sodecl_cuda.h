@@ -258,8 +258,8 @@ int sodecl_cuda_launch(sodecl_ctx *ctx, const sodecl_launch *launch, void *strea
  * orbit for RK4, num_equat + 1 otherwise) and nothing is recomputed.  The
  * default picks that when the buffer takes at most half the free device
  * memory, else ~sqrt(steps).  The context keeps the buffer for its next call
- * (sodecl_cuda_destroy frees it).  Gradients are the same bit for bit with
- * any spacing.
+ * (sodecl_cuda_release_scratch or sodecl_cuda_destroy frees it).  Gradients
+ * are the same bit for bit with any spacing.
  * Records, steps and the step size follow the context's configuration; all
  * pointers are device pointers; the launch goes on `stream`.  No
  * counterpart in the reference. */
@@ -303,6 +303,12 @@ int sodecl_cuda_kernel_info(sodecl_ctx *ctx, int *regs, int *local_bytes, int *m
  * sodecl_cuda_get_cfg). */
 int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_steps, int32_t *block,
                          int32_t *min_blocks, int32_t *division, int32_t *lanes, double *best_ms);
+
+/* Frees the device scratch a context keeps for its next call: the record
+ * buffer of runs into host memory and the adjoint's checkpoint / trajectory
+ * buffer (tens of GB for large fits).  The next call allocates again.  Waits
+ * for the context's queued work.  No counterpart in the reference. */
+int sodecl_cuda_release_scratch(sodecl_ctx *ctx);
 
 /* The context's configuration as it stands, e.g. after sodecl_cuda_autotune. */
 int sodecl_cuda_get_cfg(const sodecl_ctx *ctx, sodecl_cfg *cfg);

@@ -218,6 +218,12 @@ class Integrator:
         la.flags = flags
         N.check(N.lib.sodecl_cuda_launch(self._ctx, C.byref(la), stream), self._ctx)
 
+    def release_scratch(self):
+        """Frees the device buffers kept between calls (records of host-output
+        runs, the adjoint's trajectory or checkpoints); later calls allocate
+        them again."""
+        N.check(N.lib.sodecl_cuda_release_scratch(self._ctx), self._ctx)
+
     def close(self):
         if self._ctx:
             N.lib.sodecl_cuda_destroy(self._ctx)

@@ -1248,6 +1248,23 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
     return SODECL_OK;
 }
 
+int sodecl_cuda_release_scratch(sodecl_ctx *ctx)
+{
+    if (!ctx) return SODECL_ERR_INVALID_ARG;
+    if (!ctx->d_records && !ctx->adj_scratch) return SODECL_OK;
+    DeviceScope dev(ctx->cfg.device);
+    // the buffers may still be in use by work queued on the context's streams
+    if (ctx->stream) SODECL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->copy_stream) SODECL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->copy_stream));
+    SODECL_CUDA_TRY(ctx, cudaFree(ctx->d_records));
+    ctx->d_records = nullptr;
+    ctx->d_records_bytes = 0;
+    SODECL_CUDA_TRY(ctx, cudaFree(ctx->adj_scratch));
+    ctx->adj_scratch = nullptr;
+    ctx->adj_scratch_bytes = 0;
+    return SODECL_OK;
+}
+
 int sodecl_cuda_get_cfg(const sodecl_ctx *ctx, sodecl_cfg *cfg)
 {
     if (!ctx || !cfg) return SODECL_ERR_INVALID_ARG;

@@ -157,6 +157,35 @@ def test_adjoint_against_finite_differences_and_checkpoint_spacing():
 
 
 @pytest.mark.gpu
+def test_release_scratch_returns_the_trajectory_buffer():
+    """The whole-trajectory buffer stays with the context between calls;
+    release_scratch hands it back to the device, and the next call
+    allocates it again and gives the same gradients."""
+    torch = pytest.importorskip("torch")
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.fit import Adjoint
+
+    n, nchunks, ksteps, dt = 1 << 14, 10, 50, 1e-5
+    t0, y0, p, tg = fitting_problem(n, 3, dt=dt, nchunks=nchunks, ksteps=ksteps)
+    dev = torch.device("cuda")
+    T = lambda a: torch.tensor(a, device=dev)  # noqa: E731
+    with Integrator(system_path("oculomotor"), "rk4", orbits=n, dt=dt, tspan=(nchunks * ksteps - 0.5) * dt,
+                    ksteps=ksteps, neq=6, npar=6) as sim:
+        adj = Adjoint(sim)
+        first = adj(T(t0), T(y0), T(p), T(tg))
+        torch.cuda.synchronize()
+        held = n * nchunks * ksteps * 25 * 8  # the RK4 trajectory: state, t and three stage inputs per step
+        before = torch.cuda.mem_get_info()[0]
+        sim.release_scratch()
+        after = torch.cuda.mem_get_info()[0]
+        assert after - before >= 0.9 * held
+        sim.release_scratch()  # nothing left: a no-op
+        again = adj(T(t0), T(y0), T(p), T(tg))
+        for a, b in zip(first[:3], again[:3]):
+            assert torch.equal(a, b)
+
+
+@pytest.mark.gpu
 def test_torch_autograd_function_and_tape_overflow():
     torch = pytest.importorskip("torch")
     from sodecl_b200 import Integrator, system_path
