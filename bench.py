@@ -357,6 +357,7 @@ def main():
     if not a.no_extras and world == 1:
         extras = companions(a, n, dev, stream, peaks)
         extras["gradient"] = gradient_companion(dev)
+        extras["gradient_implicit_midpoint"] = gradient_implicit_companion(dev)
         extras["uneven_batch"] = batch_companion(dev)
         extras["uneven_batch_full"] = batch_full_companion()
         extras["stochastic_kuramoto"] = stochastic_kuramoto_companion(dev, stream)
@@ -517,6 +518,60 @@ def gradient_companion(dev, n=1 << 16, nsteps=5000, ksteps=100, dt=1e-5):
             "fd": "central, relative step 1e-6, 24 perturbed copies per orbit in one launch",
             "derivatives": "adjoint_ms: the system file's calc_vjp; adjoint_jacobians_ms: its calc_jacobian + "
                            "calc_jacobian_params; adjoint_tape_ms: reverse mode over sode_system"}
+
+
+def gradient_implicit_companion(dev, n=1 << 16, nsteps=1000, ksteps=100, dt=1e-3, newton_tol=1e-10):
+    """The same fit with implicit midpoint steps (dt 1e-3, where the model is
+    stable under it): the discrete adjoint of the implicit step taken as
+    solved exactly (one transposed solve with the full Jacobian per step)
+    against central finite differences (24 perturbed copies in one loss-only
+    launch).  Newton tolerance 1e-10 (the pass limit the reference's 1000), so
+    that the converged steps the differences see are close to the exact steps
+    the adjoint differentiates; orbits with a step stopped at the pass limit
+    are counted and left out of the comparison (their steps are not the
+    solved ones)."""
+    import torch
+
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.fit import Adjoint, finite_difference_gradient
+
+    from sodecl_b200.workloads import fitting_targets
+
+    _, y0, guess, targets = fitting_targets(n, nsteps, ksteps, dt, device=dev, solver="im", newton_tol=newton_tol)
+    kw = dict(dt=dt, tspan=(nsteps - 0.5) * dt, ksteps=ksteps, neq=6, npar=6, newton_tol=newton_tol)
+    sim = Integrator(system_path("oculomotor"), "im", orbits=n, **kw)
+    wide_sim = Integrator(system_path("oculomotor"), "im", orbits=n * 24, **kw)
+    adj, wide = Adjoint(sim), Adjoint(wide_sim)
+    T = lambda x: torch.tensor(x, device=dev)  # noqa: E731
+    t0, y0d, gd = T(np.zeros(n)), T(y0), T(guess)
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        out = []
+        for _ in range(reps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            r = fn()
+            e.record()
+            torch.cuda.synchronize()
+            out.append(s.elapsed_time(e))
+        return float(np.median(out)), r
+
+    ms_adj, (loss, gp, gy, flags) = timed(lambda: adj(t0, y0d, gd, targets))
+    ms_fd, (fp, fy) = timed(lambda: finite_difference_gradient(t0, y0d, gd, targets, wide))
+    ok = (flags == 0).cpu().numpy()
+    dp = ((gp - fp).abs().amax(1) / gp.abs().amax(1)).cpu().numpy()[ok]
+    dy = ((gy - fy).abs().amax(1) / gy.abs().amax(1)).cpu().numpy()[ok]
+    q = lambda d: {"median": float(np.median(d)), "p99": float(np.quantile(d, 0.99)),  # noqa: E731
+                   "max": float(d.max())}
+    sim.close()
+    wide_sim.close()
+    return {"solver": "im", "orbits": n, "nsteps": nsteps, "record_every": ksteps, "dt": dt,
+            "newton_tol": newton_tol, "adjoint_ms": ms_adj, "finite_difference_ms": ms_fd,
+            "speedup_vs_fd": ms_fd / ms_adj, "rel_diff_vs_fd_params": q(dp), "rel_diff_vs_fd_y0": q(dy),
+            "orbits_flagged": int((~ok).sum()), "compared": "orbits with every step converged",
+            "fd": "central, relative step 1e-6, 24 perturbed copies per orbit in one launch"}
 
 
 def tuning_steps(steps, scale=64):

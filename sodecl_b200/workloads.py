@@ -96,8 +96,10 @@ def _batch_main(a):
                           "block": block, "blocks_per_sm": bps, "lanes": b.lanes}), flush=True)
 
 
-def fitting_targets(n, nsteps, ksteps, dt, seed=55, device="cuda"):
-    """(t0, y0, guess params, targets[records, 6, n]) of the oculomotor fit."""
+def fitting_targets(n, nsteps, ksteps, dt, seed=55, device="cuda", solver="rk4", newton_tol=1e-7):
+    """(t0, y0, guess params, targets[records, 6, n]) of the oculomotor fit:
+    the trajectories of seeded true parameters (integrated with `solver`)
+    plus N(0, 1e-2) noise; the guess is within 5 % of the truth."""
     import torch
 
     from . import Integrator, system_path
@@ -106,8 +108,8 @@ def fitting_targets(n, nsteps, ksteps, dt, seed=55, device="cuda"):
     true_p = NOMINAL * rng.uniform(0.5, 1.5, (n, 6))
     guess = true_p * rng.uniform(0.95, 1.05, (n, 6))
     y0 = np.tile(Y0, (n, 1))
-    sim = Integrator(system_path("oculomotor"), "rk4", dt=dt, tspan=(nsteps - 0.5) * dt, ksteps=ksteps, neq=6,
-                     npar=6, orbits=n)
+    sim = Integrator(system_path("oculomotor"), solver, dt=dt, tspan=(nsteps - 0.5) * dt, ksteps=ksteps, neq=6,
+                     npar=6, orbits=n, newton_tol=newton_tol)
     T = lambda x: torch.tensor(x, device=device)  # noqa: E731
     rec = torch.empty((sim.num_records, 6, n), dtype=torch.float64, device=device)
     td, yd, pd = T(np.zeros(n)), T(y0), T(true_p)
