@@ -306,9 +306,18 @@ int sodecl_cuda_autotune(sodecl_ctx *ctx, int64_t sample_orbits, int32_t sample_
 
 /* Frees the device scratch a context keeps for its next call: the record
  * buffer of runs into host memory and the adjoint's checkpoint / trajectory
- * buffer (tens of GB for large fits).  The next call allocates again.  Waits
+ * buffer (tens of GB for large fits), and the record buffer that destroyed
+ * contexts left on its device (below).  The next call allocates again.  Waits
  * for the context's queued work.  No counterpart in the reference. */
 int sodecl_cuda_release_scratch(sodecl_ctx *ctx);
+
+/* A destroyed context leaves its record buffer (runs into host memory) to
+ * the next context on the same device, one buffer per device, because the
+ * reference's callers make a new manager for every call and a multi-GB
+ * free and allocation per call cost up to hundreds of milliseconds.  This
+ * frees it.  Call it before cudaDeviceReset.  No counterpart in the
+ * reference. */
+int sodecl_cuda_release_cached(int device);
 
 /* The context's configuration as it stands, e.g. after sodecl_cuda_autotune. */
 int sodecl_cuda_get_cfg(const sodecl_ctx *ctx, sodecl_cfg *cfg);

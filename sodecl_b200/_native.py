@@ -144,6 +144,7 @@ SIGNATURES = {
     "sodecl_cuda_abi_version": (C.c_int, []),
     "sodecl_cuda_device_count": (C.c_int, [C.POINTER(C.c_int)]),
     "sodecl_cuda_release_scratch": (C.c_int, [C.c_void_p]),
+    "sodecl_cuda_release_cached": (C.c_int, [C.c_int]),
     "sodecl_cuda_device_describe": (C.c_int, [C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_int),
                                               C.POINTER(C.c_int)]),
     "sodecl_cuda_launch": (C.c_int, [C.c_void_p, C.POINTER(Launch), C.c_void_p]),

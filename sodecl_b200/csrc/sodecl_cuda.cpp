@@ -200,6 +200,76 @@ size_t copy_string(const std::string &s, char *buf, size_t n)
     return s.size();
 }
 
+// One record buffer per device outlives the context that allocated it: the
+// reference's callers make a new manager per call (sodecl.py), and freeing
+// and allocating a multi-GB buffer every call was measured to take from a
+// few to several hundred milliseconds.  A destroyed context leaves its record
+// buffer here (the larger of two is kept), and the next context on the
+// device takes it if it is large enough.  sodecl_cuda_release_cached and
+// sodecl_cuda_release_scratch free it.
+constexpr int kCacheDevices = 64;
+struct RecordCache {
+    std::mutex m;
+    void *ptr[kCacheDevices] = {};
+    size_t bytes[kCacheDevices] = {};
+};
+
+RecordCache &record_cache()
+{
+    static RecordCache *cache = new RecordCache();  // never destroyed: no teardown-order hazards
+    return *cache;
+}
+
+// Takes the cached buffer of `device` if it holds `need` bytes.
+void *take_cached_records(int device, size_t need, size_t *bytes)
+{
+    if (device < 0 || device >= kCacheDevices) return nullptr;
+    RecordCache &c = record_cache();
+    std::lock_guard<std::mutex> lock(c.m);
+    if (!c.ptr[device] || c.bytes[device] < need) return nullptr;
+    void *p = c.ptr[device];
+    *bytes = c.bytes[device];
+    c.ptr[device] = nullptr;
+    c.bytes[device] = 0;
+    return p;
+}
+
+// Leaves an idle buffer of `device` (the current device) for the next
+// context, keeping the larger of it and the one already cached.
+void give_cached_records(int device, void *p, size_t bytes)
+{
+    if (!p) return;
+    if (device < 0 || device >= kCacheDevices) {
+        cudaFree(p);
+        return;
+    }
+    RecordCache &c = record_cache();
+    void *drop = p;
+    {
+        std::lock_guard<std::mutex> lock(c.m);
+        if (!c.ptr[device] || c.bytes[device] < bytes) {
+            drop = c.ptr[device];
+            c.ptr[device] = p;
+            c.bytes[device] = bytes;
+        }
+    }
+    if (drop) cudaFree(drop);
+}
+
+void release_cached_records(int device)
+{
+    if (device < 0 || device >= kCacheDevices) return;
+    RecordCache &c = record_cache();
+    void *drop = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(c.m);
+        drop = c.ptr[device];
+        c.ptr[device] = nullptr;
+        c.bytes[device] = 0;
+    }
+    if (drop) cudaFree(drop);
+}
+
 void free_buffers(sodecl_ctx *ctx)
 {
     cudaFree(ctx->d_t);
@@ -208,7 +278,7 @@ void free_buffers(sodecl_ctx *ctx)
     cudaFree(ctx->d_cnt);
     cudaFree(ctx->d_passes);
     cudaFree(ctx->d_flags);
-    cudaFree(ctx->d_records);
+    give_cached_records(ctx->cfg.device, ctx->d_records, ctx->d_records_bytes);
     ctx->d_t = ctx->d_y = ctx->d_p = ctx->d_cnt = nullptr;
     ctx->d_passes = nullptr;
     ctx->d_flags = nullptr;
@@ -744,11 +814,13 @@ int sodecl_cuda_run(sodecl_ctx *ctx, double *out, int64_t out_len)
         // the copy stream moves each group's records out while later groups run
         const size_t need = static_cast<size_t>(nrec * rec_elems) * sizeof(double);
         if (ctx->d_records_bytes < need) {
-            cudaFree(ctx->d_records);
-            ctx->d_records = nullptr;
-            ctx->d_records_bytes = 0;
-            SODECL_CUDA_TRY(ctx, cudaMalloc(&ctx->d_records, need));
-            ctx->d_records_bytes = need;
+            give_cached_records(ctx->cfg.device, ctx->d_records, ctx->d_records_bytes);
+            ctx->d_records = take_cached_records(ctx->cfg.device, need, &ctx->d_records_bytes);
+            if (!ctx->d_records) {
+                ctx->d_records_bytes = 0;
+                SODECL_CUDA_TRY(ctx, cudaMalloc(&ctx->d_records, need));
+                ctx->d_records_bytes = need;
+            }
         }
         // Pinned output: launch groups of halving size (half the record
         // intervals, a quarter, ...; the last takes the rest): each group's
@@ -1251,17 +1323,31 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
 int sodecl_cuda_release_scratch(sodecl_ctx *ctx)
 {
     if (!ctx) return SODECL_ERR_INVALID_ARG;
-    if (!ctx->d_records && !ctx->adj_scratch) return SODECL_OK;
     DeviceScope dev(ctx->cfg.device);
-    // the buffers may still be in use by work queued on the context's streams
-    if (ctx->stream) SODECL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
-    if (ctx->copy_stream) SODECL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->copy_stream));
-    SODECL_CUDA_TRY(ctx, cudaFree(ctx->d_records));
-    ctx->d_records = nullptr;
-    ctx->d_records_bytes = 0;
-    SODECL_CUDA_TRY(ctx, cudaFree(ctx->adj_scratch));
-    ctx->adj_scratch = nullptr;
-    ctx->adj_scratch_bytes = 0;
+    if (ctx->d_records || ctx->adj_scratch) {
+        // the buffers may still be in use by work queued on the context's streams
+        if (ctx->stream) SODECL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+        if (ctx->copy_stream) SODECL_CUDA_TRY(ctx, cudaStreamSynchronize(ctx->copy_stream));
+        SODECL_CUDA_TRY(ctx, cudaFree(ctx->d_records));
+        ctx->d_records = nullptr;
+        ctx->d_records_bytes = 0;
+        SODECL_CUDA_TRY(ctx, cudaFree(ctx->adj_scratch));
+        ctx->adj_scratch = nullptr;
+        ctx->adj_scratch_bytes = 0;
+    }
+    release_cached_records(ctx->cfg.device);  // and what earlier contexts left
+    return SODECL_OK;
+}
+
+int sodecl_cuda_release_cached(int device)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) {
+        cudaGetLastError();
+        return SODECL_ERR_NO_DEVICE;
+    }
+    DeviceScope dev(device);
+    release_cached_records(device);
     return SODECL_OK;
 }
 

@@ -475,6 +475,35 @@ def test_pair_stores_write_the_same_records():
         assert not (outs[0][base_off:].reshape(nchunks + 1, 6, stride)[:, :, lo:lo + m] == FILL).any()
 
 
+def test_record_buffer_passes_to_the_next_context():
+    """A destroyed context leaves its device record buffer to the next one on
+    the device (the reference's callers make a manager per call); the next
+    run allocates nothing new and gives the same records, and
+    sodecl_cuda_release_cached frees the buffer."""
+    import torch
+
+    n = 1 << 18
+    t0, y0, p = oculomotor_inputs(n, 44)
+    kw = dict(dt=1e-3, tspan=0.1, ksteps=10, neq=6, npar=6)
+    with Integrator(system_path("oculomotor"), "rk4", orbits=n, **kw) as sim:
+        sim.upload(t0, y0, p)
+        first = sim.run()
+        held = first.nbytes
+    torch.cuda.synchronize()
+    f1 = torch.cuda.mem_get_info()[0]
+    with Integrator(system_path("oculomotor"), "rk4", orbits=n, **kw) as sim:
+        sim.upload(t0, y0, p)
+        again = sim.run()
+        f2 = torch.cuda.mem_get_info()[0]
+    np.testing.assert_array_equal(again, first)
+    assert f1 - f2 < held // 2  # the state buffers only: the records came from the first context
+    f3 = torch.cuda.mem_get_info()[0]
+    N.check(N.lib.sodecl_cuda_release_cached(0))
+    f4 = torch.cuda.mem_get_info()[0]
+    assert f4 - f3 >= 0.9 * held
+    N.check(N.lib.sodecl_cuda_release_cached(0))  # nothing left: a no-op
+
+
 # --------------------------------------------------------------------------
 # the reciprocal quotient
 
