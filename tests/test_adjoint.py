@@ -130,6 +130,32 @@ def test_implicit_adjoint_matches_reference_gradient(solver, products):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("solver", ["ie", "im"])
+def test_implicit_adjoint_schedules_agree(solver):
+    """Implicit solvers: the whole-trajectory schedule and the checkpoint
+    schedules give the same loss, gradients and pass-limit flags bit for bit,
+    steps stopped at the pass limit included."""
+    torch = pytest.importorskip("torch")
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.fit import Adjoint
+
+    n, nchunks, ksteps, dt = 2000, 6, 25, 1e-3
+    sid = 3 if solver == "ie" else 4
+    t0, y0, p, tg = fitting_problem(n, 9, dt=dt, nchunks=nchunks, ksteps=ksteps, solver=sid)
+    T = lambda a: torch.tensor(a, device="cuda")  # noqa: E731
+    for max_iter in (1000, 12):  # 12 passes stop steps early (flagged)
+        sim = Integrator(system_path("oculomotor"), solver, dt=dt, tspan=(nchunks * ksteps - 0.5) * dt,
+                         ksteps=ksteps, neq=6, npar=6, orbits=n, newton_tol=1e-10, newton_max_iter=max_iter)
+        runs = [Adjoint(sim, ckpt_every=c)(T(t0), T(y0), T(p), T(tg)) for c in (0, 1, 7, 10**6)]
+        flagged = int((runs[0][3] != 0).sum())
+        assert flagged > 0 if max_iter == 12 else flagged < n
+        for r in runs[1:]:
+            for a, b in zip(r, runs[0]):
+                assert torch.equal(a, b)
+        sim.close()
+
+
+@pytest.mark.gpu
 def test_adjoint_against_finite_differences_and_checkpoint_spacing():
     torch = pytest.importorskip("torch")
     from sodecl_b200 import Integrator, system_path
