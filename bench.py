@@ -69,6 +69,7 @@ def parse():
 # the reference's own system file, staged verbatim by oracle/build.py
 REFERENCE_SYSTEM = os.path.join(REPO, "baseline", "_ref", "examples", "oculomotor.cl")
 PACKAGE_SYSTEM = os.path.join(REPO, "sodecl_b200", "systems", "oculomotor.cl")
+REFERENCE_KURAMOTO = os.path.join(REPO, "baseline", "_ref", "examples", "kuramoto.cl")
 
 
 def headline_system():
@@ -682,7 +683,10 @@ def stochastic_kuramoto_companion(dev, stream, n=1 << 18, N=32, nsteps=2000, kst
     orbit, counters orbit * 2^20, dt=0.01, a record every 200 steps, FP64 (and
     FP32).  2000 of the full configuration's 2x10^4 steps keep the default run
     short (the rate does not depend on the step count).  One thread per orbit
-    against the tuned launch (lanes per orbit for this 32-equation system)."""
+    against the tuned launch (lanes per orbit for this 32-equation system),
+    and the reference's own examples/kuramoto.cl (same arithmetic; without
+    the per-row functions lanes per orbit need, so one thread per orbit,
+    tuned)."""
     import torch
 
     from sodecl_b200 import Integrator, system_path
@@ -691,10 +695,14 @@ def stochastic_kuramoto_companion(dev, stream, n=1 << 18, N=32, nsteps=2000, kst
 
     _, th0, p, cnt = kuramoto(n, N, seed=seed, noise=True)
     out = {}
-    for name, prec, lanes, tune in (("one_thread_per_orbit_fp64", "fp64", 1, False), ("tuned_fp64", "fp64", 1, True),
-                                    ("tuned_fp32", "fp32", 1, True)):
-        sim = Integrator(system_path("kuramoto"), "se", dt=0.01, tspan=nsteps * 0.01, ksteps=ksteps, neq=N,
-                         npar=2 * N + 1, nnoi=N, orbits=n, precision=prec, lanes=lanes)
+    cases = [("one_thread_per_orbit_fp64", system_path("kuramoto"), "fp64", False),
+             ("tuned_fp64", system_path("kuramoto"), "fp64", True),
+             ("tuned_fp32", system_path("kuramoto"), "fp32", True)]
+    if os.path.isfile(REFERENCE_KURAMOTO):
+        cases.append(("reference_file_tuned_fp64", REFERENCE_KURAMOTO, "fp64", True))
+    for name, path, prec, tune in cases:
+        sim = Integrator(path, "se", dt=0.01, tspan=nsteps * 0.01, ksteps=ksteps, neq=N,
+                         npar=2 * N + 1, nnoi=N, orbits=n, precision=prec)
         choice = None
         if tune:
             sim.upload(np.zeros(n), th0, p, cnt)
