@@ -9,8 +9,10 @@ they pass every input and output as their own device buffers.
 Checked here: through the C ABI, two calls in a row (the second on a scratch
 array still holding the first call's values) give exactly what the regular
 entry point (sodecl_batch_set_items + sodecl_batch_run) gives -- bit for bit,
-the tolerance the other batch tests use.  This file is collected last so a
-run that stops at the first failure has already run every other test."""
+the tolerance the other batch tests use -- and sampled orbits of every class
+match the CPU oracle within the floor-based tolerance of tests/parity.py.
+This file is collected last so a run that stops at the first failure has
+already run every other test."""
 import ctypes as C
 
 import numpy as np
@@ -99,6 +101,15 @@ def test_noalloc_batch_run_matches_regular_entry_point_twice():
         np.testing.assert_array_equal(c_d.cpu().numpy(), c_ref)
         np.testing.assert_array_equal(passes_d.cpu().numpy(), passes_ref)
         np.testing.assert_array_equal(flags_d.cpu().numpy(), flags_ref)
+
+    # and against the CPU oracle, not only against the library's other entry
+    # point: sampled orbits of every class at their own step counts
+    from test_batch import assert_batch_final_states_match_oracle
+
+    widths = np.array([CLASSES[c][2] for c in cls])
+    y_orbits = np.split(y_d.cpu().numpy(), np.cumsum(widths)[:-1])
+    assert_batch_final_states_match_oracle(CLASSES, cls, steps, t0, y0, p, counters, t_d.cpu().numpy(), y_orbits,
+                                           c_d.cpu().numpy(), 8, 12)
 
 
 @pytest.mark.gpu
