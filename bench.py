@@ -357,12 +357,14 @@ def main():
     # rank's GPU while rank 0 alone works
     if not a.no_extras and world == 1:
         extras = companions(a, n, dev, stream, peaks)
+        # the ceiling of right-hand sides made of sines (the Kuramoto lines)
+        sin_peaks = {prec: sodecl_b200.sin_peak(prec, device=local_rank)[0] for prec in ("fp64", "fp32")}
         extras["gradient"] = gradient_companion(dev)
         extras["gradient_implicit_midpoint"] = gradient_implicit_companion(dev)
-        extras["uneven_batch"] = batch_companion(dev)
-        extras["uneven_batch_full"] = batch_full_companion()
-        extras["stochastic_kuramoto"] = stochastic_kuramoto_companion(dev, stream)
-        extras["small_kuramoto"] = small_kuramoto_companion(dev, stream)
+        extras["uneven_batch"] = batch_companion(dev, sin_peaks)
+        extras["uneven_batch_full"] = batch_full_companion(sin_peaks)
+        extras["stochastic_kuramoto"] = stochastic_kuramoto_companion(dev, stream, sin_peaks)
+        extras["small_kuramoto"] = small_kuramoto_companion(dev, stream, sin_peaks)
         try:
             extras["adaptive"] = adaptive_companion(a, n, dev, stream)
         except Exception as exc:  # a companion line only: the headline stands without it
@@ -584,7 +586,38 @@ def tuning_steps(steps, scale=64):
     return np.maximum(1, steps // scale)
 
 
-def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
+def sine_roofline(sines, seconds, peak, basis):
+    """Roofline block of a Kuramoto line: sine evaluations per second against
+    the measured throughput of the math library's sin (sodecl_cuda_sin_peak,
+    fastest of 7 launches at full occupancy)."""
+    achieved = sines / seconds
+    return {"bound": "sin", "achieved": achieved, "peak": peak, "unit": "sines/s", "frac": achieved / peak,
+            "sines": basis, "peak_source": "measured on this GPU: sodecl_cuda_sin_peak (eight independent sums of "
+                                           "sin(x_k - y) per thread, fastest of 7 launches)"}
+
+
+def kuramoto_sines(classes, cls, steps, passes):
+    """Sine evaluations of an uneven sweep's Kuramoto orbits: N^2 per
+    right-hand side (Euler one per step, RK4 four), and N^2 per Newton pass of
+    implicit Euler (a pass evaluates every row's N terms; where it also takes
+    the band from the same sincos, or the Jacobian's cosines, those are not
+    counted: a lower bound).  The oculomotor orbits evaluate no sine."""
+    total = 0
+    for k, (system, solver, neq, npar, dt) in enumerate(classes):
+        if system != "kuramoto":
+            continue
+        m = cls == k
+        per = {"euler": int(steps[m].sum()), "rk4": 4 * int(steps[m].sum()), "ie": int(passes[m].sum())}[solver]
+        total += per * neq * neq
+    return total
+
+
+SINE_BASIS_BATCH = ("Kuramoto orbits only: N^2 sines per right-hand side (Euler 1, RK4 4 per step) and per implicit "
+                    "Euler Newton pass (sincos counted once, cosines of the Jacobian not counted); oculomotor work "
+                    "not counted: a lower bound")
+
+
+def batch_companion(dev, sin_peaks, n=1 << 15, max_steps=10000, seed=4):
     """The uneven-sweep shape: orbits mixing Kuramoto N in {4, 16, 64} and the
     oculomotor model, solver per orbit in {Euler, RK4, implicit Euler}, step
     counts log-uniform in [10^2, max_steps], FP64.  The full configuration is
@@ -618,6 +651,8 @@ def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
         times.append(b.run(graph=True))
     batch_ms = float(np.median(times))
     useful = int(steps.sum())
+    _, _, _, passes, _ = b.results()
+    sines = kuramoto_sines(classes, cls, steps, passes)
     # padded: per class, every orbit runs the class's longest orbit, with the
     # lanes per orbit the tuner chose for the class
     tuned_lanes = b.lanes
@@ -644,10 +679,11 @@ def batch_companion(dev, n=1 << 15, max_steps=10000, seed=4):
             "orbit_steps": useful, "batch_ms": batch_ms, "value": useful / (batch_ms * 1e-3), "unit": METRIC,
             "tuned_launch": {"block": block, "blocks_per_sm": bps}, "padded_per_class_ms": padded_ms,
             "speedup_vs_padded": padded_ms / batch_ms, "registers": b.kernel_info()["registers"],
-            "lanes_per_class": b.lanes}
+            "lanes_per_class": b.lanes,
+            "roofline": sine_roofline(sines, batch_ms * 1e-3, sin_peaks["fp64"], SINE_BASIS_BATCH)}
 
 
-def batch_full_companion(n=1 << 18, max_steps=100000, seed=4):
+def batch_full_companion(sin_peaks, n=1 << 18, max_steps=100000, seed=4):
     """The uneven sweep at its configured size: 2^18 orbits, step counts
     log-uniform in [10^2, 10^5] (3.8e9 orbit-steps), the same 12 classes, in
     one persistent launch (CUDA graph), after the tuner has chosen lanes per
@@ -668,16 +704,17 @@ def batch_full_companion(n=1 << 18, max_steps=100000, seed=4):
     b.set_items(cls, steps, np.zeros(n), y0, p)
     b.set_launch(block, bps)
     ms = b.run(graph=True)
-    _, _, _, _, flags = b.results()
+    _, _, _, passes, flags = b.results()
     useful = int(steps.sum())
+    sines = kuramoto_sines(classes, cls, steps, passes)
     return {"orbits": n, "classes": len(classes), "steps": "log-uniform [100, %d]" % max_steps,
             "orbit_steps": useful, "batch_ms": ms, "value": useful / (ms * 1e-3), "unit": METRIC,
             "tuned_launch": {"block": block, "blocks_per_sm": bps}, "lanes_per_class": b.lanes,
             "registers": b.kernel_info()["registers"], "orbits_flagged": int((flags != 0).sum()),
-            "launches_timed": 1}
+            "launches_timed": 1, "roofline": sine_roofline(sines, ms * 1e-3, sin_peaks["fp64"], SINE_BASIS_BATCH)}
 
 
-def stochastic_kuramoto_companion(dev, stream, n=1 << 18, N=32, nsteps=2000, ksteps=200, seed=3):
+def stochastic_kuramoto_companion(dev, stream, sin_peaks, n=1 << 18, N=32, nsteps=2000, ksteps=200, seed=3):
     """Stochastic Kuramoto by Euler-Maruyama: N=32 phases, 2^18 orbits,
     K ~ U(0,5), omega ~ N(0,1) shared, additive noise sigma ~ U(0,0.5) per
     orbit, counters orbit * 2^20, dt=0.01, a record every 200 steps, FP64 (and
@@ -686,7 +723,8 @@ def stochastic_kuramoto_companion(dev, stream, n=1 << 18, N=32, nsteps=2000, kst
     against the tuned launch (lanes per orbit for this 32-equation system),
     and the reference's own examples/kuramoto.cl (same arithmetic; without
     the per-row functions lanes per orbit need, so one thread per orbit,
-    tuned)."""
+    tuned).  Each line carries its roofline against the measured sine
+    throughput of its precision."""
     import torch
 
     from sodecl_b200 import Integrator, system_path
@@ -706,7 +744,10 @@ def stochastic_kuramoto_companion(dev, stream, n=1 << 18, N=32, nsteps=2000, kst
         choice = None
         if tune:
             sim.upload(np.zeros(n), th0, p, cnt)
-            choice = sim.autotune(sample_orbits=1 << 15, sample_steps=100)
+            # trials on every orbit: with one thread per orbit a register cap
+            # pays only when the launch has many waves, which a sample of
+            # 2^15 orbits (a fraction of one wave) does not show
+            choice = sim.autotune(sample_orbits=n, sample_steps=50)
         td, yd, pd, cd = [torch.tensor(x, device=dev) for x in (np.zeros(n), th0, p, cnt)]
         rec = torch.empty((sim.num_records, N, n), dtype=torch.float64, device=dev)
         ms = []
@@ -725,7 +766,10 @@ def stochastic_kuramoto_companion(dev, stream, n=1 << 18, N=32, nsteps=2000, kst
         info = sim.kernel_info()
         out[name] = {"value": n * nsteps / (np.mean(ms) * 1e-3), "unit": METRIC, "ms": float(np.mean(ms)),
                      "precision": prec, "launch": choice or {"lanes": 1, "block": 128},
-                     "registers": info["registers"], "local_bytes": info["local_bytes"]}
+                     "registers": info["registers"], "local_bytes": info["local_bytes"],
+                     "roofline": sine_roofline(n * nsteps * N * N, np.mean(ms) * 1e-3, sin_peaks[prec],
+                                               "N^2 = %d sines per orbit-step (one right-hand side); the noise's "
+                                               "Threefry words, logarithms and square roots not counted" % (N * N))}
         sim.close()
         del rec
         torch.cuda.empty_cache()
@@ -870,7 +914,7 @@ def adaptive_companion(a, n, dev, stream):
     return out
 
 
-def small_kuramoto_companion(dev, stream):
+def small_kuramoto_companion(dev, stream, sin_peaks):
     """The plain CPU-sized case: Kuramoto N=8, 1024 orbits, K ~ U(0,5) per orbit,
     omega ~ N(0,1) shared, theta0 ~ U(0, 2 pi), explicit Euler, dt 0.05, 1000
     steps, a record every 10 (101 records), FP64.  One launch; at this size it
@@ -908,7 +952,9 @@ def small_kuramoto_companion(dev, stream):
                 ms.append(s.elapsed_time(e))
         sim.close()
         out[name] = {"ms": float(np.mean(ms)), "value": n * nsteps / (np.mean(ms) * 1e-3),
-                     "launch": choice or {"lanes": 1, "block": 128}}
+                     "launch": choice or {"lanes": 1, "block": 128},
+                     "roofline": sine_roofline(n * nsteps * N * N, np.mean(ms) * 1e-3, sin_peaks["fp64"],
+                                               "N^2 = %d sines per orbit-step (one right-hand side)" % (N * N))}
     return out
 
 

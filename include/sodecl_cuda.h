@@ -462,6 +462,15 @@ int sodecl_cuda_division_check_f32(int device, int64_t pairs, uint64_t seed, int
  * that launch's time. */
 int sodecl_cuda_fma_peak(int device, int32_t precision, double *fma_per_s, double *ms);
 
+/* Throughput microbenchmark of the math library's sin in FP64 (precision 0)
+ * or FP32 (1): eight independent sums of sin(x_k - y) per thread on every SM,
+ * with arguments within a few units of zero, the coupling term of the
+ * Kuramoto right-hand side.  Timed as sodecl_cuda_fma_peak; writes sines
+ * per second and that launch's time.  It is the ceiling of a right-hand side
+ * made of sine evaluations, as the FMA rate is of plain arithmetic.  No
+ * counterpart in the reference (a measurement of this library's own). */
+int sodecl_cuda_sin_peak(int device, int32_t precision, double *sin_per_s, double *ms);
+
 #ifdef __cplusplus
 }
 #endif

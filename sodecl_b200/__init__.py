@@ -14,7 +14,7 @@ module of this package that needs no GPU (the seeded workload generators in
 """
 import importlib
 
-__all__ = ["Integrator", "fma_peak", "noise_stream", "system_path"]
+__all__ = ["Integrator", "fma_peak", "noise_stream", "sin_peak", "system_path"]
 
 
 def __getattr__(name):

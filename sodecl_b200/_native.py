@@ -177,6 +177,7 @@ SIGNATURES = {
     "sodecl_batch_destroy": (None, [_P]),
     "sodecl_batch_run_noalloc": (C.c_int, [_P, C.POINTER(BatchIO), _P]),
     "sodecl_cuda_fma_peak": (C.c_int, [C.c_int, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    "sodecl_cuda_sin_peak": (C.c_int, [C.c_int, C.c_int32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
 
 

@@ -265,3 +265,12 @@ def fma_peak(precision="fp64", device=0):
     prec = N.FP32 if precision == "fp32" else N.FP64
     N.check(N.lib.sodecl_cuda_fma_peak(device, prec, C.byref(rate), C.byref(ms)))
     return rate.value, ms.value
+
+
+def sin_peak(precision="fp64", device=0):
+    """Measured sine evaluations per second of the math library's sin (FP64 or
+    FP32) at full occupancy, arguments within a few units of zero."""
+    rate, ms = C.c_double(), C.c_double()
+    prec = N.FP32 if precision == "fp32" else N.FP64
+    N.check(N.lib.sodecl_cuda_sin_peak(device, prec, C.byref(rate), C.byref(ms)))
+    return rate.value, ms.value

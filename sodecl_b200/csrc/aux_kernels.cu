@@ -161,11 +161,60 @@ __global__ void __launch_bounds__(256) fma_chains_kernel(T *sink, int iters, T a
     if (s == (T)-12345.0) sink[blockIdx.x * blockDim.x + threadIdx.x] = s;  // never true; keeps the chains live
 }
 
+// Sines at full occupancy: eight independent sums of sin(x_k - y) per thread,
+// the coupling term of a Kuramoto row, with arguments within a few units of
+// zero (where phases that have drifted apart by a few radians put them).
+template <class T>
+__global__ void __launch_bounds__(256) sin_sums_kernel(T *sink, int iters, T step)
+{
+    T x[8], acc[8];
+    const T y0 = (T)(threadIdx.x % 64) * (T)0.01;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        x[k] = y0 + (T)k * (T)0.7 - (T)2.5;
+        acc[k] = (T)0;
+    }
+    T y = (T)0;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] += sin(x[k] - y);
+        y += step;
+    }
+    const T s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+    if (s == (T)-12345.0) sink[blockIdx.x * blockDim.x + threadIdx.x] = s;  // never true; keeps the sums live
+}
+
 struct DeviceGuard {
     int prev = -1;
     explicit DeviceGuard(int dev) { if (cudaGetDevice(&prev) != cudaSuccess) prev = -1; cudaSetDevice(dev); }
     ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
 };
+
+// The fastest of kTrials timed launches of `launch` (after two warm-up
+// launches of `warm`), in ms; err gets the first CUDA error.
+template <class Warm, class Launch>
+float fastest_launch_ms(Warm warm, Launch launch, cudaError_t *err)
+{
+    constexpr int kTrials = 7;
+    cudaEvent_t e[kTrials + 1];
+    for (auto &ev : e) cudaEventCreate(&ev);
+    warm();
+    launch();
+    cudaEventRecord(e[0]);
+    for (int k = 0; k < kTrials; ++k) {
+        launch();
+        cudaEventRecord(e[k + 1]);
+    }
+    *err = cudaEventSynchronize(e[kTrials]);
+    float ms = 0.f;
+    for (int k = 0; k < kTrials; ++k) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, e[k], e[k + 1]);
+        if (k == 0 || t < ms) ms = t;
+    }
+    for (auto &ev : e) cudaEventDestroy(ev);
+    return ms;
+}
 
 template <class T>
 int run_fma_peak(int device, double *fma_per_s, double *ms_out)
@@ -176,33 +225,40 @@ int run_fma_peak(int device, double *fma_per_s, double *ms_out)
     const int block = 256;
     const int blocks = prop.multiProcessorCount * 8;
     const int iters = 1 << 15;
-    // the fastest of kTrials timed launches (about 20 ms each for FP64), after
-    // two warm-up launches
-    constexpr int kTrials = 7;
     T *sink = nullptr;
     if (cudaMalloc(&sink, sizeof(T) * (size_t)blocks * block) != cudaSuccess) { cudaGetLastError(); return SODECL_ERR_OUT_OF_MEMORY; }
-    cudaEvent_t e[kTrials + 1];
-    for (auto &ev : e) cudaEventCreate(&ev);
     const T a = (T)0.999999, b = (T)1e-7;
-    fma_chains_kernel<T><<<blocks, block>>>(sink, iters / 8, a, b);  // warm-up
-    fma_chains_kernel<T><<<blocks, block>>>(sink, iters, a, b);
-    cudaEventRecord(e[0]);
-    for (int k = 0; k < kTrials; ++k) {
-        fma_chains_kernel<T><<<blocks, block>>>(sink, iters, a, b);
-        cudaEventRecord(e[k + 1]);
-    }
-    cudaError_t err = cudaEventSynchronize(e[kTrials]);
-    float ms = 0.f;
-    for (int k = 0; k < kTrials; ++k) {
-        float t = 0.f;
-        cudaEventElapsedTime(&t, e[k], e[k + 1]);
-        if (k == 0 || t < ms) ms = t;
-    }
-    for (auto &ev : e) cudaEventDestroy(ev);
+    // the fastest of 7 timed launches (about 20 ms each for FP64)
+    cudaError_t err = cudaSuccess;
+    const float ms = fastest_launch_ms([&] { fma_chains_kernel<T><<<blocks, block>>>(sink, iters / 8, a, b); },
+                                       [&] { fma_chains_kernel<T><<<blocks, block>>>(sink, iters, a, b); }, &err);
     cudaFree(sink);
     if (err != cudaSuccess) { cudaGetLastError(); return SODECL_ERR_CUDA; }
     const double fmas = (double)blocks * block * (double)iters * 4.0 * 8.0;
     if (fma_per_s) *fma_per_s = fmas / (ms * 1e-3);
+    if (ms_out) *ms_out = ms;
+    return SODECL_OK;
+}
+
+template <class T>
+int run_sin_peak(int device, double *sin_per_s, double *ms_out)
+{
+    DeviceGuard guard(device);
+    cudaDeviceProp prop{};
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { cudaGetLastError(); return SODECL_ERR_NO_DEVICE; }
+    const int block = 256;
+    const int blocks = prop.multiProcessorCount * 8;
+    const int iters = 2048;  // about 20 ms a launch in FP64
+    T *sink = nullptr;
+    if (cudaMalloc(&sink, sizeof(T) * (size_t)blocks * block) != cudaSuccess) { cudaGetLastError(); return SODECL_ERR_OUT_OF_MEMORY; }
+    const T step = (T)2e-3;
+    cudaError_t err = cudaSuccess;
+    const float ms = fastest_launch_ms([&] { sin_sums_kernel<T><<<blocks, block>>>(sink, iters / 8, step); },
+                                       [&] { sin_sums_kernel<T><<<blocks, block>>>(sink, iters, step); }, &err);
+    cudaFree(sink);
+    if (err != cudaSuccess) { cudaGetLastError(); return SODECL_ERR_CUDA; }
+    const double sines = (double)blocks * block * (double)iters * 8.0;
+    if (sin_per_s) *sin_per_s = sines / (ms * 1e-3);
     if (ms_out) *ms_out = ms;
     return SODECL_OK;
 }
@@ -329,5 +385,14 @@ extern "C" int sodecl_cuda_fma_peak(int device, int32_t precision, double *fma_p
     if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) { cudaGetLastError(); return SODECL_ERR_NO_DEVICE; }
     if (precision == SODECL_FP64) return run_fma_peak<double>(device, fma_per_s, ms);
     if (precision == SODECL_FP32) return run_fma_peak<float>(device, fma_per_s, ms);
+    return SODECL_ERR_INVALID_ARG;
+}
+
+extern "C" int sodecl_cuda_sin_peak(int device, int32_t precision, double *sin_per_s, double *ms)
+{
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) { cudaGetLastError(); return SODECL_ERR_NO_DEVICE; }
+    if (precision == SODECL_FP64) return run_sin_peak<double>(device, sin_per_s, ms);
+    if (precision == SODECL_FP32) return run_sin_peak<float>(device, sin_per_s, ms);
     return SODECL_ERR_INVALID_ARG;
 }
