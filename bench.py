@@ -356,19 +356,28 @@ def main():
     # companions on single-GPU runs only: under torchrun they would hold every
     # rank's GPU while rank 0 alone works
     if not a.no_extras and world == 1:
-        extras = companions(a, n, dev, stream, peaks)
+        def line(name, fn):
+            # a companion line only: an error takes its place, the headline stands
+            try:
+                extras[name] = fn()
+            except Exception as exc:
+                extras[name] = {"error": "%s: %s" % (type(exc).__name__, exc)}
+                try:
+                    torch.cuda.synchronize()
+                    torch.cuda.empty_cache()
+                except Exception:
+                    pass
+
+        line("companions", lambda: companions(a, n, dev, stream, peaks)["companions"])
         # the ceiling of right-hand sides made of sines (the Kuramoto lines)
         sin_peaks = {prec: sodecl_b200.sin_peak(prec, device=local_rank)[0] for prec in ("fp64", "fp32")}
-        extras["gradient"] = gradient_companion(dev)
-        extras["gradient_implicit_midpoint"] = gradient_implicit_companion(dev)
-        extras["uneven_batch"] = batch_companion(dev, sin_peaks)
-        extras["uneven_batch_full"] = batch_full_companion(sin_peaks)
-        extras["stochastic_kuramoto"] = stochastic_kuramoto_companion(dev, stream, sin_peaks)
-        extras["small_kuramoto"] = small_kuramoto_companion(dev, stream, sin_peaks)
-        try:
-            extras["adaptive"] = adaptive_companion(a, n, dev, stream)
-        except Exception as exc:  # a companion line only: the headline stands without it
-            extras["adaptive"] = {"error": "%s: %s" % (type(exc).__name__, exc)}
+        line("gradient", lambda: gradient_companion(dev))
+        line("gradient_implicit_midpoint", lambda: gradient_implicit_companion(dev))
+        line("uneven_batch", lambda: batch_companion(dev, sin_peaks))
+        line("uneven_batch_full", lambda: batch_full_companion(sin_peaks))
+        line("stochastic_kuramoto", lambda: stochastic_kuramoto_companion(dev, stream, sin_peaks))
+        line("small_kuramoto", lambda: small_kuramoto_companion(dev, stream, sin_peaks))
+        line("adaptive", lambda: adaptive_companion(a, n, dev, stream))
 
     cpu = None
     if rank == 0 and world == 1:
