@@ -19,6 +19,9 @@ Workload (one "step" = one full integration of one batch of orbits):
             microbenchmark (2 flops per FMA).
   cpu_baseline  the reference's kernels compiled as C (oracle/_ref), OpenMP over
             all host cores, on an orbit subsample of the same workload.
+  parity    the timed launch's records of that subsample against the CPU
+            baseline's (relative error over elements finite in both, and the
+            count of elements finite in only one).
 
 --impl reference runs only that CPU implementation of the path (rank 0), on
 the cpu_baseline leg's sample: the first 2^15 orbits with all 10^4 steps per
@@ -146,7 +149,8 @@ class ClockSampler:
 
 
 def cpu_reference_rate(n, a, cores, kind_pref="reference"):
-    """orbit-steps/s of the CPU implementation on the first n orbits."""
+    """(orbit-steps/s, seconds, kind, records) of the CPU implementation on the
+    first n orbits."""
     from oracle.oracle import Oracle, ReferenceBuild
 
     t0, y0, p = workload(n, 0)
@@ -159,9 +163,27 @@ def cpu_reference_rate(n, a, cores, kind_pref="reference"):
         impl, kind = Oracle("oculomotor"), "port"
         fn = lambda: impl.run(solver, t0, y0, p, **kw)  # noqa: E731
     t = time.perf_counter()
-    fn()
+    res = fn()
     secs = time.perf_counter() - t
-    return n * a.nsteps / secs, secs, kind
+    return n * a.nsteps / secs, secs, kind, res.records
+
+
+def records_error(got, want):
+    """The GPU's records against the CPU implementation's on the same orbits:
+    per element |got - want| / (|want| + 1e-3 S_e), S_e the largest finite
+    |value| of equation e, over elements finite in both; and the count of
+    elements finite in one and not the other."""
+    fin_w, fin_g = np.isfinite(want), np.isfinite(got)
+    both = fin_w & fin_g
+    scale = np.max(np.where(fin_w, np.abs(want), 0.0), axis=(0, 2), keepdims=True)
+    den = np.abs(want) + 1e-3 * scale + 1e-300
+    err = np.where(both, np.abs(np.where(both, got, 0.0) - np.where(both, want, 0.0)) / den, 0.0)
+    e = err[both]
+    return {"max_rel_err": float(e.max()) if e.size else 0.0,
+            "p99_rel_err": float(np.quantile(e, 0.99)) if e.size else 0.0,
+            "median_rel_err": float(np.median(e)) if e.size else 0.0,
+            "elements_finite_in_both": int(both.sum()), "elements": int(both.size),
+            "finite_mismatch": int(np.count_nonzero(fin_w != fin_g))}
 
 
 def run_reference_arm(a, rank):
@@ -179,7 +201,7 @@ def run_reference_arm(a, rank):
     secs = []
     kind = None
     for _ in range(a.steps):
-        _, sec, kind = cpu_reference_rate(n, a, cores)
+        _, sec, kind, _ = cpu_reference_rate(n, a, cores)
         secs.append(sec)
     ms = float(np.mean(secs)) * 1e3
     value = n * a.nsteps / (ms * 1e-3)
@@ -282,6 +304,8 @@ def main():
     ms = float(np.mean(launch_ms))
     ms = max_over_ranks(ms, dist, dev)
     rec_last = rec_d[-1].cpu().numpy()
+    # the records of the orbits the CPU baseline integrates, checked against it below
+    rec_sample = rec_d[:, :, :min(a.cpu_orbits, n)].cpu().numpy() if rank == 0 and world == 1 else None
     nan_fraction = float(np.mean(~np.isfinite(rec_last).all(axis=0)))
     value = world * n * a.nsteps / (ms * 1e-3)
 
@@ -379,13 +403,18 @@ def main():
         line("small_kuramoto", lambda: small_kuramoto_companion(dev, stream, sin_peaks))
         line("adaptive", lambda: adaptive_companion(a, n, dev, stream))
 
-    cpu = None
+    cpu = parity = None
     if rank == 0 and world == 1:
         cores = os.cpu_count() or 1
-        v, secs, kind = cpu_reference_rate(a.cpu_orbits, a, cores)
+        v, secs, kind, cpu_records = cpu_reference_rate(min(a.cpu_orbits, n), a, cores)
+        parity = records_error(rec_sample, cpu_records)
+        parity.update({"vs": "the CPU baseline's records (%s) of the same %d orbits, all %d records"
+                             % ("the reference's kernels compiled as C" if kind == "reference" else "the oracle",
+                                rec_sample.shape[2], rec_sample.shape[0]),
+                       "fmad": "GPU with FMA contraction (the library's default), CPU without"})
         cpu = {"value": v, "unit": METRIC, "cores": cores, "kind": kind,
-               "sample": "%d of %d orbits, all %d steps, records every %d (%.1f s)" % (a.cpu_orbits, n, a.nsteps,
-                                                                                     a.ksteps, secs)}
+               "sample": "%d of %d orbits, all %d steps, records every %d (%.1f s)" % (min(a.cpu_orbits, n), n,
+                                                                                     a.nsteps, a.ksteps, secs)}
     info = sim.kernel_info()
     if rank == 0:
         launch_info = {"parallelism": "orbits sharded, %d per GPU" % n, "block": sim.cfg.local_group_size or 128,
@@ -397,6 +426,7 @@ def main():
                "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f64" if a.precision == "fp64" else "f32", "data": "synthetic",
                "config": config_dict(a, n), "launch": launch_info, "roofline": roofline, "cpu_baseline": cpu,
+               "parity": parity,
                "e2e": e2e, "e2e_dropin": e2e_dropin, "gpu_launches": a.steps, "clocks": clocks.summary(), "wall_s_timed_region": wall,
                "launch_ms": launch_ms}
         out.update(extras)
