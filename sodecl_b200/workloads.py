@@ -18,6 +18,8 @@ Shapes (all inputs seeded; no dataset is involved):
   adjoint-oculomotor    loss and gradient (sodecl_cuda_adjoint) of the oculomotor
                         RK4 fit: targets from seeded true parameters + N(0, 1e-2)
                         noise, gradient at parameters within +-5 % of them; dt 1e-5
+  peaks                 the measured ceilings: FMA issue rate and sine throughput,
+                        FP64 and FP32 (sodecl_cuda_fma_peak, sodecl_cuda_sin_peak)
 """
 from __future__ import annotations
 
@@ -147,7 +149,7 @@ def _adjoint_main(a):
 def _parse():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("case", help="oculomotor-<solver> | stochastic-kuramoto | kuramoto-<solver> | uneven-batch | "
-                                 "adjoint-oculomotor")
+                                 "adjoint-oculomotor | peaks")
     ap.add_argument("--orbits", type=int, default=1 << 15)
     ap.add_argument("--nsteps", type=int, default=200)
     ap.add_argument("--ksteps", type=int, default=100)
@@ -177,6 +179,15 @@ def main():
 
     a = _parse()
     n = a.orbits
+    if a.case == "peaks":
+        from . import fma_peak, sin_peak
+
+        for prec in ("fp64", "fp32"):
+            fma, fms = fma_peak(prec)
+            sines, sms = sin_peak(prec)
+            print(json.dumps({"case": a.case, "precision": prec, "fma_per_s": fma, "fma_ms": fms, "sin_per_s": sines,
+                              "sin_ms": sms}), flush=True)
+        return
     if a.case == "adjoint-oculomotor":
         return _adjoint_main(a)
     if a.case == "uneven-batch":
