@@ -32,6 +32,8 @@ offset by rank): weak scaling, no collective on the data path.
 from __future__ import annotations
 
 import argparse
+import contextlib
+import ctypes
 import json
 import os
 import subprocess
@@ -73,6 +75,25 @@ def parse():
 REFERENCE_SYSTEM = os.path.join(REPO, "baseline", "_ref", "examples", "oculomotor.cl")
 PACKAGE_SYSTEM = os.path.join(REPO, "sodecl_b200", "systems", "oculomotor.cl")
 REFERENCE_KURAMOTO = os.path.join(REPO, "baseline", "_ref", "examples", "kuramoto.cl")
+
+
+@contextlib.contextmanager
+def stdout_to_stderr():
+    """Sends what native code prints to standard output (the C++ manager's
+    'Compute results runtime' line, as the reference prints it) to standard
+    error, so that the bench's standard output carries its JSON line alone.
+    The C library's buffers are flushed before the descriptor is restored."""
+    sys.stdout.flush()
+    libc = ctypes.CDLL(None)
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        libc.fflush(None)
+        sys.stdout.flush()
+        os.dup2(saved, 1)
+        os.close(saved)
 
 
 def headline_system():
@@ -379,7 +400,8 @@ def main():
     # ---------------- the drop-in path end to end (single-GPU runs)
     e2e_dropin = None
     if not a.no_e2e and world == 1:
-        e2e_dropin = dropin_e2e(a, n, t0, y0, p, rec_last)
+        with stdout_to_stderr():
+            e2e_dropin = dropin_e2e(a, n, t0, y0, p, rec_last)
 
     # ---------------- companions: stable step, fp32, implicit midpoint
     extras = {}
@@ -407,6 +429,7 @@ def main():
         line("uneven_batch_full", lambda: batch_full_companion(sin_peaks))
         line("stochastic_kuramoto", lambda: stochastic_kuramoto_companion(dev, stream, sin_peaks))
         line("small_kuramoto", lambda: small_kuramoto_companion(dev, stream, sin_peaks))
+        line("readme_case", readme_case_companion)
         line("adaptive", lambda: adaptive_companion(a, n, dev, stream))
 
     cpu = parity = None
@@ -960,6 +983,60 @@ def adaptive_companion(a, n, dev, stream):
            "nan_fraction_final": float(np.mean(~np.isfinite(last).all(axis=0)))}
     sim.close()
     return out
+
+
+# The reference's one published figure (its README): "Compute results runtime:
+# 0.0690873 sec." for examples/kuramoto_euler_stochastic.py on an Intel Core
+# i7-4790K at 4.00 GHz, Intel OpenCL CPU runtime, local group size 8.
+README_PUBLISHED_S = 0.0690873
+
+
+def readme_case_companion(reps=5):
+    """The run the reference publishes a time for: its README's
+    examples/kuramoto_euler_stochastic.py -- Kuramoto N=3 by Euler-Maruyama,
+    2 orbits, dt 0.05, tspan 50, a record every 40 steps (1000 steps, 26
+    records), phases U(-3.1416, 3.1416), K 0.2, omega U(0.2, 0.4), noise
+    amplitudes U(0.01, 0.03) (seeded here; the script draws them unseeded) --
+    on the reference's own examples/kuramoto.cl, through the reference's
+    Python entry point on this library (sodecl_b200.sodecl.sodecl, a new
+    manager per call, as the script makes).  'compute_results_runtime_s' is
+    what the reference's line of that name times (the run loop: launches and
+    record copies, sodeclmgr.cpp:951-1020), from this library's own timing of
+    sodecl_cuda_run; 'call_s' is the whole call with the program from the
+    cache (the reference's 'Simulation execution time', 0.589 s there,
+    includes its OpenCL build)."""
+    from sodecl_b200 import Integrator, system_path
+    from sodecl_b200.sodecl import sodecl
+
+    path = REFERENCE_KURAMOTO if os.path.isfile(REFERENCE_KURAMOTO) else system_path("kuramoto")
+    orbits, nequat, nnoi, dt, tspan, ksteps = 2, 3, 3, 0.05, 50.0, 40
+    rng = np.random.default_rng(12)
+    initx = rng.uniform(-3.1416, 3.1416, (orbits, nequat))
+    params = np.concatenate([np.full((orbits, 1), 0.2), rng.uniform(0.2, 0.4, (orbits, nequat)),
+                             rng.uniform(0.01, 0.03, (orbits, nequat))], axis=1)
+    # the run loop alone, as the reference's "Compute results runtime" line times it
+    sim = Integrator(path, "se", dt=dt, tspan=tspan, ksteps=ksteps, neq=nequat, npar=params.shape[1], nnoi=nnoi,
+                     orbits=orbits)
+    loop_ms = []
+    for _ in range(reps + 1):
+        sim.upload(np.zeros(orbits), initx, params)
+        sim.run()
+        loop_ms.append(sim.last_run_ms()[1])
+    sim.close()
+    # the whole call through the reference's entry point
+    call_s = []
+    with stdout_to_stderr():
+        for _ in range(reps + 1):
+            w = time.perf_counter()
+            t, res = sodecl(0, 0, path, initx, params, 0, orbits, nequat, nnoi, dt, tspan, ksteps, 0)
+            call_s.append(time.perf_counter() - w)
+    runtime_s = float(np.median(loop_ms[1:])) * 1e-3
+    return {"system_file": "reference examples/kuramoto.cl" if path == REFERENCE_KURAMOTO else "package kuramoto.cl",
+            "orbits": orbits, "N": nequat, "solver": "Euler-Maruyama", "dt": dt, "tspan": tspan, "record_every": ksteps,
+            "records": int(res.shape[1]), "compute_results_runtime_s": runtime_s,
+            "call_s": float(np.median(call_s[1:])), "published_s": README_PUBLISHED_S,
+            "published_hardware": "Intel Core i7-4790K @ 4.00 GHz, Intel OpenCL CPU runtime (the reference's README)",
+            "speedup_vs_published": README_PUBLISHED_S / runtime_s}
 
 
 def small_kuramoto_companion(dev, stream, sin_peaks):
