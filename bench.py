@@ -21,7 +21,10 @@ Workload (one "step" = one full integration of one batch of orbits):
             all host cores, on an orbit subsample of the same workload.
   parity    the timed launch's records of that subsample against the CPU
             baseline's: relative error over the orbits finite in both runs,
-            and counts of the orbits that diverge in both or in one only.
+            and counts of the orbits that diverge in both or in one only;
+            beside it the floor, the same measure between the CPU baseline
+            and the oracle compiled with FMA contraction, and whether the
+            error is within 10x the floor (the GPU parity tests' rule).
 
 --impl reference runs only that CPU implementation of the path (rank 0), on
 the cpu_baseline leg's sample: the first 2^15 orbits with all 10^4 steps per
@@ -187,6 +190,22 @@ def cpu_reference_rate(n, a, cores, kind_pref="reference"):
     res = fn()
     secs = time.perf_counter() - t
     return n * a.nsteps / secs, secs, kind, res.records
+
+
+def parity_floor(n, a, cores, cpu_records):
+    """The same measure between two CPU builds of the same computation on the
+    same orbits: the CPU baseline's records against the oracle compiled with
+    FMA contraction.  At an unstable step the orbits that stay finite still
+    amplify last-bit differences, and this is how far they carry them."""
+    from oracle.oracle import Oracle
+
+    t0, y0, p = workload(n, 0)
+    solver = {"rk4": 2, "euler": 1, "ie": 3, "im": 4}[a.solver]
+    fma = Oracle("oculomotor", "fp64fma").run(solver, t0, y0, p, neq=6, npar=6, dt=a.dt, ksteps=a.ksteps,
+                                              nchunks=a.nsteps // a.ksteps, nthreads=cores).records
+    out = records_error(fma, cpu_records)
+    out["vs"] = "the oracle compiled with FMA contraction against the CPU baseline"
+    return out
 
 
 def records_error(got, want):
@@ -438,6 +457,9 @@ def main():
         v, secs, kind, cpu_records = cpu_reference_rate(min(a.cpu_orbits, n), a, cores)
         try:
             parity = records_error(rec_sample, cpu_records)
+            parity["floor"] = parity_floor(min(a.cpu_orbits, n), a, cores, cpu_records)
+            if "max_rel_err" in parity and "max_rel_err" in parity["floor"]:
+                parity["within_10x_floor"] = bool(parity["max_rel_err"] <= max(1e-12, 10 * parity["floor"]["max_rel_err"]))
         except Exception as exc:  # a check beside the measurement: the line stands without it
             parity = {"error": "%s: %s" % (type(exc).__name__, exc)}
         parity.update({"vs": "the CPU baseline's records (%s) of the same %d orbits, all %d records"
