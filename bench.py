@@ -490,7 +490,7 @@ def main():
         dist.destroy_process_group()
 
 
-def dropin_e2e(a, n, t0, y0, p, rec_last, reps=3):
+def dropin_e2e(a, n, t0, y0, p, rec_last, reps=5):
     """The headline through the reference's Python entry point on this
     library, sodecl_b200.sodecl.sodecl(platform, device, system file, initx,
     params, solver, orbits, nequat, nnoise, dt, tspan, ksteps, local size):
