@@ -44,3 +44,38 @@ def test_reference_arm_maps_no_library_code():
     mapped = [m for m in probe["mapped"] if m.startswith(REPO)]
     assert not [m for m in mapped if "sodecl_b200" in m], mapped
     assert any("oracle/_ref/libref_oculomotor_rk4.so" in m for m in mapped)
+
+
+def test_bench_parity_measure():
+    """The bench's parity block: relative error over the orbits finite in both
+    runs, diverging orbits counted; and its CPU-to-CPU floor on a small sample
+    of the headline's orbits at the stable step (the reference's kernels
+    against the oracle built with FMA contraction: every orbit finite in both,
+    differing in the last bits)."""
+    sys.path.insert(0, REPO)
+    import numpy as np
+
+    import bench
+
+    rng = np.random.default_rng(0)
+    want = rng.uniform(1, 2, (3, 2, 5))
+    got = want * (1 + 1e-12)
+    want[1, 0, 3] = np.nan                 # orbit 3 diverges in the CPU run only
+    got[2, 1, 4] = want[2, 1, 4] = np.inf  # orbit 4 diverges in both
+    r = bench.records_error(got, want)
+    assert (r["orbits"], r["orbits_finite_in_both"], r["orbits_diverging_in_both"], r["orbits_diverging_in_one"]) \
+        == (5, 3, 1, 1)
+    assert 0.9e-12 < r["max_rel_err"] < 1.1e-12
+
+    if not os.path.exists(os.path.join(REPO, "oracle", "_ref", "libref_oculomotor_rk4.so")):
+        pytest.skip("the reference's kernels are not built")
+    saved = sys.argv
+    sys.argv = ["bench.py", "--nsteps", "300", "--dt", "1e-5"]
+    try:
+        a = bench.parse()
+    finally:
+        sys.argv = saved
+    _, _, kind, rec = bench.cpu_reference_rate(64, a, 2)
+    assert kind == "reference" and rec.shape == (4, 6, 64)
+    floor = bench.parity_floor(64, a, 2, rec)
+    assert floor["orbits_finite_in_both"] == 64 and 0 < floor["max_rel_err"] < 1e-9
