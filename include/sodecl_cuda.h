@@ -218,7 +218,11 @@ int sodecl_cuda_device_describe(int device, char *buf, size_t n, int *major, int
  * first row is record rec_first.  Runs record intervals
  * [chunk_begin, chunk_end), storing each interval's starting state, and the
  * final state as record chunk_end if write_final.  newton_passes/flags
- * (nullable) accumulate.  The context must be compiled; no upload needed. */
+ * (nullable) accumulate.  The context must be compiled; no upload needed.
+ * Every buffer must be memory the context's device can access (its own
+ * device memory, managed memory or pinned host memory): anything else, such
+ * as a pageable host array, is refused with SODECL_ERR_INVALID_ARG before
+ * any launch. */
 typedef struct sodecl_launch {
     double *t;
     double *y;
@@ -261,8 +265,8 @@ int sodecl_cuda_launch(sodecl_ctx *ctx, const sodecl_launch *launch, void *strea
  * (sodecl_cuda_release_scratch or sodecl_cuda_destroy frees it).  Gradients
  * are the same bit for bit with any spacing.
  * Records, steps and the step size follow the context's configuration; all
- * pointers are device pointers; the launch goes on `stream`.  No
- * counterpart in the reference. */
+ * pointers are device pointers (checked as for sodecl_cuda_launch); the
+ * launch goes on `stream`.  No counterpart in the reference. */
 typedef struct sodecl_adjoint_io {
     const double *t0;       /* [n] */
     const double *y0;       /* [n][num_equat] */

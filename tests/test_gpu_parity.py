@@ -590,3 +590,36 @@ def test_autotune_keeps_results():
         np.testing.assert_array_equal(y, y0)  # tuning ran on copies
         got = sim.run()
     np.testing.assert_array_equal(got, want)
+
+
+def test_device_entry_points_refuse_host_buffers():
+    """sodecl_cuda_launch and sodecl_cuda_adjoint take device pointers.  A
+    pageable host array handed to them by mistake is refused on the host,
+    before any launch (a kernel would fault on it), and the context stays
+    usable: the next launch with device buffers gives the records the
+    host-output run gives."""
+    torch = pytest.importorskip("torch")
+    from sodecl_b200.fit import Adjoint
+
+    n = 64
+    t0, y0, p = oculomotor_inputs(n, 9)
+    kw = dict(dt=1e-5, tspan=5e-4, ksteps=10, neq=6, npar=6)
+    with Integrator(system_path("oculomotor"), "rk4", orbits=n, **kw) as sim:
+        sim.upload(t0, y0, p)
+        want = sim.run()
+        dev = torch.device("cuda")
+        td, yd, pd = (torch.tensor(x, device=dev) for x in (t0, y0, p))
+        rec = torch.empty((sim.num_records, 6, n), dtype=torch.float64, device=dev)
+        host_y = np.ascontiguousarray(y0)
+        with pytest.raises(N.SodeclError, match="not memory this device can access"):
+            sim.launch(t=td.data_ptr(), y=host_y.ctypes.data, params=pd.data_ptr(), records=rec.data_ptr())
+        host_rec = np.empty((sim.num_records, 6, n))
+        with pytest.raises(N.SodeclError, match="not memory this device can access"):
+            sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(), records=host_rec.ctypes.data)
+        targets = torch.tensor(want, device=dev)
+        with pytest.raises(N.SodeclError, match="not memory this device can access"):
+            Adjoint(sim)(td, torch.tensor(y0), pd, targets)   # y0 left in host memory
+        sim.launch(t=td.data_ptr(), y=yd.data_ptr(), params=pd.data_ptr(), records=rec.data_ptr(),
+                   stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(rec.cpu().numpy(), want)
