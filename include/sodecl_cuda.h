@@ -415,9 +415,11 @@ size_t sodecl_batch_last_error(const sodecl_batch *b, char *buf, size_t n);
  * need scratch for the permutation).  Put long orbits first for the same
  * load balance.
  *
- * Inputs are not validated on the host beyond null checks: every pointer but
- * class_count must be device memory the caller owns, sized for the counts
- * in class_count; a step count of zero or less takes no step and leaves that
+ * Inputs are not validated on the host beyond null checks and the kind of
+ * memory (as for sodecl_cuda_launch: memory the device cannot access is
+ * refused): every pointer but class_count must be device memory the caller
+ * owns, sized for the counts in class_count, whose contents the host never
+ * reads; a step count of zero or less takes no step and leaves that
  * orbit's state unchanged. */
 typedef struct sodecl_batch_io {
     double *t;                  /* device, [n] in/out */

@@ -16,6 +16,7 @@
 #include <numeric>
 
 #include "batch_internal.hpp"
+#include "device_memory.hpp"
 
 namespace {
 
@@ -93,6 +94,13 @@ extern "C" int sodecl_batch_run_noalloc(sodecl_batch *b, const sodecl_batch_io *
     }
     CurrentDevice dev(b->device);
     if (!dev.ok) return fail(b, SODECL_ERR_NO_DEVICE, "no-alloc run: cannot select the device");
+    for (const void *p : {static_cast<const void *>(io->t), static_cast<const void *>(io->y),
+                          static_cast<const void *>(io->params), static_cast<const void *>(io->counters),
+                          static_cast<const void *>(io->nsteps), static_cast<const void *>(io->newton_passes),
+                          static_cast<const void *>(io->flags)})
+        if (!sodecl_b200::kernel_can_access(p, b->device))
+            return fail(b, SODECL_ERR_INVALID_ARG, "no-alloc run: a buffer is not memory this device can access "
+                                                   "(device, managed or pinned host memory)");
 
     // first call on this device: load the batch program and look up the
     // scratch array's address

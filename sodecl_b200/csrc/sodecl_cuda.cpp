@@ -25,6 +25,7 @@
 #include <thread>
 #include <vector>
 
+#include "device_memory.hpp"
 #include "program.hpp"
 
 using sodecl_b200::Program;
@@ -391,27 +392,6 @@ bool staging_ready(StagingPool &pool)
         pool.slots.push_back(p);
     }
     return true;
-}
-
-// Whether a kernel on `device` may dereference p: memory of that device,
-// managed memory, or pinned host memory (mapped into the device's address
-// space).  Pageable host memory, another device's memory or an address CUDA
-// does not know would fault the kernel, so the entry points that take device
-// pointers refuse them.  A null p is for the caller to judge.
-bool kernel_can_access(const void *p, int device)
-{
-    if (!p) return true;
-    cudaPointerAttributes attr{};
-    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    switch (attr.type) {
-    case cudaMemoryTypeDevice: return attr.device == device;
-    case cudaMemoryTypeManaged: return true;
-    case cudaMemoryTypeHost: return attr.devicePointer != nullptr;
-    default: return false;
-    }
 }
 
 // Whether the system file has the per-row functions lanes per orbit need
@@ -982,7 +962,7 @@ int sodecl_cuda_launch(sodecl_ctx *ctx, const sodecl_launch *l, void *stream)
                           static_cast<const void *>(l->params), static_cast<const void *>(l->counters),
                           static_cast<const void *>(l->records), static_cast<const void *>(l->newton_passes),
                           static_cast<const void *>(l->flags)})
-        if (!kernel_can_access(p, ctx->cfg.device))
+        if (!sodecl_b200::kernel_can_access(p, ctx->cfg.device))
             return ctx->fail(SODECL_ERR_INVALID_ARG, "launch: a buffer is not memory this device can access "
                                                      "(device, managed or pinned host memory)");
     DeviceArgs a{};
@@ -1220,7 +1200,7 @@ int sodecl_cuda_adjoint(sodecl_ctx *ctx, const sodecl_adjoint_io *io, void *stre
                           static_cast<const void *>(io->params), static_cast<const void *>(io->targets),
                           static_cast<const void *>(io->loss), static_cast<const void *>(io->grad_params),
                           static_cast<const void *>(io->grad_y0), static_cast<const void *>(io->flags)})
-        if (!kernel_can_access(p, ctx->cfg.device))
+        if (!sodecl_b200::kernel_can_access(p, ctx->cfg.device))
             return ctx->fail(SODECL_ERR_INVALID_ARG, "adjoint: a buffer is not memory this device can access "
                                                      "(device, managed or pinned host memory)");
     const int tape = io->tape_entries > 0 ? io->tape_entries : 256;

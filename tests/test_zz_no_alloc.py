@@ -156,3 +156,38 @@ def test_noalloc_step_count_below_zero_takes_no_step():
     np.testing.assert_array_equal(c_d.cpu().numpy(), c_ref)
     np.testing.assert_array_equal(passes_d.cpu().numpy(), passes_ref)
     assert (passes_d.cpu().numpy()[negative] == 0).all()
+
+
+@pytest.mark.gpu
+def test_noalloc_refuses_host_buffers():
+    """A pageable host array in place of a device buffer is refused on the
+    host, before the scratch is touched or anything is launched; the next call
+    with device buffers runs and matches the regular entry point."""
+    torch = pytest.importorskip("torch")
+    if N.device_count() < 1:
+        pytest.fail("no CUDA device")
+    per_class = [32, 32, 16, 16, 16, 16]
+    cls, steps, t0, y0, p, counters = class_grouped_items(per_class, 7)
+    ref = build_batch()
+    ref.set_items(cls, steps, t0, y0, p, counters)
+    ref.run(graph=False)
+    _, y_ref, _, _, _ = ref.results()
+
+    b = build_batch()
+    dev = torch.device("cuda", 0)
+    t_d = torch.tensor(t0, device=dev)
+    y_d = torch.tensor(np.concatenate(y0), device=dev)
+    p_d = torch.tensor(np.concatenate(p), device=dev)
+    c_d = torch.tensor(counters, device=dev)
+    s_d = torch.tensor(steps, device=dev)
+    counts = np.array(per_class, dtype=np.int64)
+    host_steps = np.ascontiguousarray(steps)
+    stream = C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+    io = N.BatchIO()
+    io.t, io.y, io.params, io.counters = t_d.data_ptr(), y_d.data_ptr(), p_d.data_ptr(), c_d.data_ptr()
+    io.nsteps, io.class_count = host_steps.ctypes.data, counts.ctypes.data
+    assert N.lib.sodecl_batch_run_noalloc(b._b, C.byref(io), stream) == N.ERR_INVALID_ARG
+    io.nsteps = s_d.data_ptr()
+    assert N.lib.sodecl_batch_run_noalloc(b._b, C.byref(io), stream) == N.OK
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(y_d.cpu().numpy(), np.concatenate(y_ref))
