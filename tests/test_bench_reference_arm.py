@@ -79,3 +79,24 @@ def test_bench_parity_measure():
     assert kind == "reference" and rec.shape == (4, 6, 64)
     floor = bench.parity_floor(64, a, 2, rec)
     assert floor["orbits_finite_in_both"] == 64 and 0 < floor["max_rel_err"] < 1e-9
+
+
+def test_bench_keeps_native_prints_off_stdout():
+    """The C++ manager prints the reference's 'Compute results runtime' line
+    to standard output; inside bench.stdout_to_stderr it goes to standard
+    error (C buffers flushed), so the bench's standard output is its JSON line
+    alone."""
+    code = r"""
+import ctypes, sys
+sys.argv = ["bench.py"]
+sys.path.insert(0, %(repo)r)
+import bench
+with bench.stdout_to_stderr():
+    ctypes.CDLL(None).printf(b"Compute results runtime: 0.1 sec.\n")
+    print("python inside")
+print('{"metric": "x"}', flush=True)
+""" % {"repo": REPO}
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120, cwd=REPO)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout == '{"metric": "x"}\n'
+    assert "Compute results runtime" in out.stderr and "python inside" in out.stderr
