@@ -11,7 +11,7 @@ namespace sodecl_b200 {
 // managed memory, or pinned host memory (mapped into the device's address
 // space).  Pageable host memory, another device's memory or an address CUDA
 // does not know would fault the kernel, so those entry points refuse them.
-// Allocates nothing.  A null p is for the caller to judge.
+// Allocates nothing.  Whether a null p is allowed is for the caller to decide.
 inline bool kernel_can_access(const void *p, int device)
 {
     if (!p) return true;
